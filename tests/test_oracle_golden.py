@@ -1,0 +1,242 @@
+"""Pin the CPU oracle against the reference's own outputs and known answers.
+
+The fixtures under tests/golden/ were produced by the reference's TorchCvdv
+(complex128, CPU) by ``tests/golden/make_golden.py``.  The known-answer tests
+restate the checks of the reference's ``tests/test_core.py``,
+``tests/test_measurement_ground_truth.py`` and ``tests/test_wigner_and_husimi.py``
+against the oracle.
+"""
+
+import math
+import os
+
+import numpy as np
+import pytest
+
+from oracle.cvdv_oracle import OracleCvdv
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+PI = np.pi
+
+
+def _load(name):
+    return dict(np.load(os.path.join(GOLD, name)))
+
+
+GATES = _load("gates.npz")
+READ = _load("readouts.npz")
+C1 = _load("c1.npz")
+SEP = _load("separable.npz")
+
+CASE_NAMES = sorted({k.split("__")[0] for k in GATES})
+
+# method name (CudaCvdv API) -> oracle call
+CALLS = {
+    "d": lambda o, r, b: o.displacement(r, complex(b).real, complex(b).imag),
+    "cd": lambda o, t, c, q, a: o.cond_displacement(t, c, q, complex(a).real, complex(a).imag),
+    "ftQ2P": lambda o, r: o.ft_q2p(r),
+    "ftP2Q": lambda o, r: o.ft_p2q(r),
+    "sheer": lambda o, r, t: o.phase_x2(r, t),
+    "phaseCubic": lambda o, r, t: o.phase_x3(r, t),
+    "r": lambda o, r, th: o.rotation(r, th),
+    "cr": lambda o, t, c, q, th: o.cond_rotation(t, c, q, th),
+    "s": lambda o, r, rr: o.squeeze(r, rr),
+    "cs": lambda o, t, c, q, rr: o.cond_squeeze(t, c, q, rr),
+    "bs": lambda o, a, b, th: o.beam_splitter(a, b, th),
+    "cbs": lambda o, a, b, c, q, th: o.cond_beam_splitter(a, b, c, q, th),
+    "q1q2": lambda o, a, b, c: o.q1q2(a, b, c),
+    "h": lambda o, r, k: o.hadamard(r, k),
+    "x": lambda o, r, k: o.pauli_rotation(r, k, 0, PI),
+    "y": lambda o, r, k: o.pauli_rotation(r, k, 1, PI),
+    "z": lambda o, r, k: o.pauli_rotation(r, k, 2, PI),
+    "rx": lambda o, r, k, t: o.pauli_rotation(r, k, 0, t),
+    "ry": lambda o, r, k, t: o.pauli_rotation(r, k, 1, t),
+    "rz": lambda o, r, k, t: o.pauli_rotation(r, k, 2, t),
+    "p": lambda o, r: o.parity(r),
+    "cp": lambda o, t, c, q: o.cparity(t, c, q),
+    "swap": lambda o, a, b: o.swap(a, b),
+}
+
+# the same sequences the fixture generator ran
+from tests.golden.cases import GATE_CASES  # noqa: E402
+
+
+# TorchCvdv.q1q2 builds q1[:, None] * q2[None, :] and reshapes it onto the
+# register axes; with reg1 > reg2 and unequal sizes that reshape scrambles the
+# matrix (src/torchCvdv.py, q1q2).  The CUDA kernel (gates.cuh:213-231) applies
+# exp(i c x_{reg1} x_{reg2}); the oracle follows the kernel, so for this case the
+# check is against that formula written out directly.
+TORCH_DIVERGES = {"q1q2_rev"}
+
+
+def rel_err(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.mark.parametrize("name,qubits,seq", GATE_CASES, ids=[c[0] for c in GATE_CASES])
+def test_gate_vs_reference_torch(name, qubits, seq):
+    o = OracleCvdv(qubits)
+    o.set_state(GATES[f"{name}__in"])
+    for meth, args in seq:
+        CALLS[meth](o, *args)
+    ref = GATES[f"{name}__out"]
+    if name in TORCH_DIVERGES:
+        assert rel_err(o.get_state(), ref) > 1e-3  # the reshape bug is visible
+        (_, (r1, r2, c)), = seq
+        x1, x2 = o.grid(r1), o.grid(r2)
+        psi = GATES[f"{name}__in"].reshape(o.dims)
+        fac = np.exp(1j * c * np.multiply.outer(x2, x1))  # axes (reg2, reg1) = (0, 1)
+        ref = (psi * fac).reshape(-1)
+    assert rel_err(o.get_state(), ref) < 1e-12, name
+
+
+def test_c1_circuit_vs_reference_torch():
+    o = OracleCvdv([1, 10])
+    o.init_from_separable([C1["reg0"], C1["reg1"]])
+    # TorchCvdv normalises at init; the CUDA path does not (context.cu:75-115)
+    assert abs(o.get_norm() - 1.0) < 1e-12
+    np.testing.assert_allclose(o.get_state(), C1["init"], rtol=0, atol=1e-14)
+    o.hadamard(0, 0)
+    o.cond_displacement(1, 0, 0, 1.5, 0.0)
+    o.rotation(1, 0.3)
+    o.squeeze(1, 0.2)
+    o.hadamard(0, 0)
+    assert rel_err(o.get_state(), C1["state"]) < 1e-12
+    np.testing.assert_allclose(o.m(0), C1["m0"], atol=1e-13)
+    np.testing.assert_allclose(o.m(1), C1["m1"], atol=1e-13)
+    W = o.wigner(1)
+    N, dx = 1024, o.dx[1]
+    dp = PI / (N * dx)
+    x = (np.arange(N) - (N - 1) / 2) * dx
+    p = (np.arange(N) - N / 2) * dp
+    Wc = W[np.ix_(np.abs(p) <= 5.0, np.abs(x) <= 5.0)]
+    assert Wc.shape == (255, 128)
+    np.testing.assert_allclose(Wc, C1["wigner_b5"], atol=1e-13)
+    # Husimi: the CUDA route (overlap + circulant Gaussian) vs TorchCvdv's
+    # direct window; the reference's own consistency tolerance is 1e-3.
+    Q = o.husimi(1)
+    dpq = 2 * PI / (N * dx)
+    pq = (np.arange(N) - N / 2) * dpq
+    Qc = Q[np.ix_(np.abs(pq) <= 5.0, np.abs(x) <= 5.0)]
+    np.testing.assert_allclose(Qc, C1["husimi_torch_b5"], atol=1e-6)
+
+
+def test_marginals_vs_reference_torch():
+    o = OracleCvdv([2, 3, 4])
+    o.set_state(READ["m_state"])
+    for key, regs in (("m_0", (0,)), ("m_1", (1,)), ("m_2", (2,)), ("m_20", (2, 0)),
+                      ("m_012", (0, 1, 2)), ("m_10", (1, 0))):
+        np.testing.assert_allclose(o.m(*regs), READ[key], atol=1e-15, err_msg=key)
+
+
+def test_photon_number_vs_reference_torch():
+    o = OracleCvdv([7])
+    o.set_state(READ["n_state"])
+    assert abs(o.photon_number(0) - float(READ["n_value"])) < 1e-12
+
+
+def test_wigner_vs_reference_torch():
+    o = OracleCvdv([6, 1])
+    o.set_state(READ["w_state"])
+    np.testing.assert_allclose(o.wigner(0), READ["w_wigner"], atol=1e-14)
+    np.testing.assert_allclose(o.husimi(0), READ["w_husimi_torch"], atol=2e-3)
+    o3 = OracleCvdv([2, 5, 2])
+    o3.set_state(READ["w3_state"])
+    np.testing.assert_allclose(o3.wigner(1), READ["w3_wigner"], atol=1e-14)
+    # For a random state on a 32-point grid the two Husimi routes differ (the
+    # CUDA route's Gaussian window is circulant, TorchCvdv's is not), so only
+    # the total mass is compared there.
+    assert abs(o3.husimi(1).sum() - READ["w3_husimi_torch"].sum()) / READ["w3_husimi_torch"].sum() < 0.05
+
+
+# ---------------------------------------------------------------- known answers
+def _grid(nq):
+    N = 1 << nq
+    dx = math.sqrt(2 * PI / N)
+    return (np.arange(N) - (N - 1) / 2) * dx, dx
+
+
+def _coherent(nq, alpha):
+    """Coherent state on the grid (the reference's SeparableState.setCoherent,
+    restated: pi^-1/4 sqrt(dx) exp(-(x-q0)^2/2) exp(i(p0 x - p0 q0/2)))."""
+    x, dx = _grid(nq)
+    q0, p0 = math.sqrt(2) * alpha.real, math.sqrt(2) * alpha.imag
+    return (PI ** -0.25) * math.sqrt(dx) * np.exp(-0.5 * (x - q0) ** 2) * np.exp(1j * (p0 * x - p0 * q0 / 2))
+
+
+def test_ft_numpy_restatement_known_answer():
+    """Momentum marginal after ftQ2P equals the reference test's numpy
+    restatement (tests/test_measurement_ground_truth.py:47-60,123-145)."""
+    nq = 8
+    for alpha in (1j, 0.5 + 1.5j, -0.4 + 1.0j, 2.0j):
+        psi = _coherent(nq, alpha)
+        o = OracleCvdv([nq])
+        o.set_state(psi)
+        o.ft_q2p(0)
+        x, dx = _grid(nq)
+        N = 1 << nq
+        c = PI * (N - 1) / (N * dx)
+        ref = np.fft.fft(psi * np.exp(1j * c * x)) / math.sqrt(N) * np.exp(1j * c * x)
+        np.testing.assert_allclose(np.abs(o.get_state()) ** 2, np.abs(ref) ** 2, atol=1e-14)
+
+
+def test_identities_known_answer():
+    """Identities of the reference's tests/test_core.py on the oracle."""
+    rng = np.random.default_rng(7)
+    # D(a)|0> = |a>
+    a = complex(rng.uniform(-2, 2), rng.uniform(-2, 2))
+    o = OracleCvdv([10])
+    o.set_state(_coherent(10, 0j))
+    o.displacement(0, a.real, a.imag)
+    assert abs(o.get_fidelity([_coherent(10, a)]) - 1) < 1e-10
+    # CD commutator: Rz(4xy) D(-iy) CD(-x) D(iy) CD(x) = I
+    x, y = 0.37, -0.61
+    o = OracleCvdv([1, 10])
+    plus = np.array([1, 1]) / math.sqrt(2)
+    vac = _coherent(10, 0j)
+    o.init_from_separable([plus, vac])
+    o.cond_displacement(1, 0, 0, x, 0)
+    o.displacement(1, 0, y)
+    o.cond_displacement(1, 0, 0, -x, 0)
+    o.displacement(1, 0, -y)
+    o.pauli_rotation(0, 0, 2, 4 * x * y)
+    assert abs(o.get_fidelity([plus, vac]) - 1) < 1e-10
+    # R(theta)|a> = |a e^{-i theta}>
+    th = 2.2
+    o = OracleCvdv([10])
+    o.set_state(_coherent(10, 3.0 + 0j))
+    o.rotation(0, th)
+    assert abs(o.get_fidelity([_coherent(10, 3.0 * np.exp(-1j * th))]) - 1) < 1e-10
+    # FT keeps Fock states (checked with a Gaussian = Fock 0)
+    o = OracleCvdv([10])
+    o.set_state(vac)
+    o.ft_q2p(0)
+    assert abs(o.get_fidelity([vac]) - 1) < 1e-10
+
+
+def test_closed_form_phase_space():
+    """Closed-form W and Q of a coherent state (tests/test_core.py:241-339)."""
+    nq, alpha = 8, 1.0 + 0.5j
+    o = OracleCvdv([nq])
+    o.set_state(_coherent(nq, alpha))
+    x, dx = _grid(nq)
+    N = 1 << nq
+    q0, p0 = math.sqrt(2) * alpha.real, math.sqrt(2) * alpha.imag
+    pw = (np.arange(N) - N / 2) * (PI / (N * dx))
+    X, P = np.meshgrid(x, pw)
+    np.testing.assert_allclose(o.wigner(0), (dx / PI) * np.exp(-(X - q0) ** 2 - (P - p0) ** 2), atol=1e-2)
+    ph = (np.arange(N) - N / 2) * (2 * PI / (N * dx))
+    X, P = np.meshgrid(x, ph)
+    Q = o.husimi(0)
+    np.testing.assert_allclose(Q, (1 / PI) * np.exp(-0.5 * (X - q0) ** 2 - 0.5 * (P - p0) ** 2), atol=5e-3)
+    assert np.all(Q >= -1e-10)
+    # photon number of a coherent state
+    o2 = OracleCvdv([nq])
+    o2.set_state(_coherent(nq, 1.5 + 1.0j))
+    assert abs(o2.photon_number(0) - abs(1.5 + 1.0j) ** 2) < 1e-2
+
+
+def test_coherent_restatement_matches_reference_setter():
+    """The helper above equals the reference SeparableState.setCoherent output."""
+    for a in (1.0, 1.5 + 0.8j, -0.5 + 2.0j):
+        np.testing.assert_allclose(_coherent(6, complex(a)), SEP[f"coherent_6_{a}"], atol=1e-15)
