@@ -1,0 +1,343 @@
+"""Benchmark: the CV-to-DV state-transfer circuit at 2^28 amplitudes.
+
+Workload (one step): the 42 gates of the 14-round state-transfer circuit
+(H, conditional displacement, Rz per round) on a resident 2^28-amplitude state
+([1]*14 + [14] registers), complex128 (the reference's arithmetic).  The state
+(4 GiB) is 32x the 126 MB L2, so no L2 flush is needed between steps.
+
+  value      gates/s on the device-resident state (CUDA events on the library's
+             stream, max over ranks), whole job
+  e2e        gates/s through the public API with host buffers: separable
+             register arrays from pinned host memory -> initStateVector ->
+             state preparation -> 42 gates -> the 14 qubit marginals to the host
+  roofline   the dominant kernel (the FFT pass) from per-launch CUDA events
+             taken inside the timed region, against the measured HBM peak
+  cpu_baseline  the CPU oracle (numpy/scipy restatement of the reference's
+             decompositions) on a bounded sample, rank 0 at N=1 only
+
+--impl reference times the CPU oracle (the reference's own implementation is
+Python that cannot be shipped here; its CUDA library needs cuTENSOR) on the
+same workload, one gate per step.
+
+Multi-GPU: replicas only (the path does not shard); every rank runs its own
+copy of the circuit and value sums the ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "cuda-cvdv_b200"))
+sys.path.insert(0, ROOT)
+
+METRIC = "gates/s (CV-to-DV state transfer, 2^28 amplitudes)"
+UNIT = "gates/s"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.3)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(nm)
+            except Exception:
+                continue
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------- CPU oracle
+def oracle_mode_state(circ):
+    """Mode register after the preparation gates, computed on the mode alone
+    (the initial state is a product, so the prepared state is too)."""
+    from oracle.cvdv_oracle import OracleSim
+    from cvdv_b200 import workloads as W
+    q = circ["qubits"][-1]
+    m = OracleSim([q])
+    sep = W.separable_arrays(circ)
+    m.init_from_separable([sep.register_arrays[-1].numpy()])
+    mode = len(circ["qubits"]) - 1
+    for meth, args in circ["prep"]:
+        if args[0] == mode:
+            getattr(m, meth)(0, *args[1:])
+    return sep, m.get_state()
+
+
+def cpu_oracle_gates(circ, gate_indices, threads):
+    """Time the oracle on the full-size state for the listed gates; returns
+    (seconds per gate list, gates timed)."""
+    import numpy as np
+    from oracle.cvdv_oracle import OracleSim
+    sep, mode = oracle_mode_state(circ)
+    o = OracleSim(circ["qubits"], workers=threads)
+    arrays = [a.numpy() for a in sep.register_arrays[:-1]] + [mode]
+    o.init_from_separable(arrays)
+    times = []
+    for gi in gate_indices:
+        meth, args = circ["gates"][gi % len(circ["gates"])]
+        t0 = time.perf_counter()
+        getattr(o, meth)(*args)
+        times.append(time.perf_counter() - t0)
+    del o
+    np.zeros(1)
+    return times
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    from cvdv_b200 import workloads as W
+    threads = os.cpu_count() or 1
+    circ = W.state_transfer()
+    # one gate per step, cycling through the circuit; warm-up gates are untimed
+    n = args.warmup + args.steps
+    times = cpu_oracle_gates(circ, list(range(n)), threads)
+    timed = times[args.warmup:]
+    sec = sum(timed)
+    value = len(timed) / sec
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sec / len(timed),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+        "data": "synthetic (seeded circuit, seed 2)",
+        "config": {"workload": "state_transfer [1]*14+[14], 2^28 amplitudes, complex128",
+                   "step": "one gate of the circuit (cycling), CPU oracle"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{len(timed)} gates of the 42-gate circuit at full size "
+                                   f"(numpy elementwise single-threaded, scipy FFT on {threads} threads)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- GPU arm
+def run_gpu(args, world, rank, local):
+    import numpy as np
+    import torch
+    from cvdv_b200 import CudaCvdv, _lib
+    from cvdv_b200 import workloads as W
+
+    torch.cuda.set_device(local)
+    L = _lib.load()
+    circ = W.state_transfer()
+    G = len(circ["gates"])
+    hbm, peak_kind = peaks()
+    out = {}
+
+    def timed_run(precision):
+        sim = CudaCvdv(circ["qubits"], precision=precision, check_errors=True)
+        sim.initStateVector(W.separable_arrays(circ, device="cuda"))
+        W.apply(sim, circ["prep"])
+        sim.synchronize()
+        stream = torch.cuda.ExternalStream(L.cvdvGetStream(sim.ctx))
+        for _ in range(args.warmup):
+            W.apply(sim, circ["gates"])
+            L.cvdvFlush(sim.ctx)
+        sim.synchronize()
+        barrier(world)
+        torch.cuda.synchronize()
+        L.cvdvSetTiming(sim.ctx, 1)
+        _lib.kernel_stats(sim.ctx)  # reset
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        n0 = L.cvdvLaunchCount()
+        clk = Clocks(local)
+        clk.start()
+        e0.record(stream)
+        for _ in range(args.steps):
+            W.apply(sim, circ["gates"])
+            L.cvdvFlush(sim.ctx)
+        e1.record(stream)
+        e1.synchronize()
+        clocks = clk.stop()
+        launches = L.cvdvLaunchCount() - n0
+        ms = e0.elapsed_time(e1) / args.steps
+        stats = _lib.kernel_stats(sim.ctx)
+        L.cvdvSetTiming(sim.ctx, 0)
+        torch.cuda.synchronize()
+        barrier(world)
+        ms = max_over_ranks(ms, world)
+        norm = sim.m()
+        del sim
+        torch.cuda.empty_cache()
+        return ms, stats, launches, clocks, norm
+
+    ms, stats, launches, clocks, norm = timed_run("complex128")
+    n_amp = 1 << sum(circ["qubits"])
+    fft_ms, fft_n = stats["fft_pass"]
+    per_launch_ms = fft_ms / max(fft_n, 1)
+    # algorithmic bytes per FFT launch: the transform's one logical read+write of
+    # the state (2 * 2^n * 16 B), split over its passes (2 passes for 2^14)
+    passes = 2
+    alg_bytes = 2 * n_amp * 16 / passes
+    achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9
+    total_kernel_ms = sum(v[0] for v in stats.values())
+    value = G * world / (ms * 1e-3)
+
+    # ---- e2e through the public API with host buffers
+    sep_host = W.separable_arrays(circ, device="cpu")
+    for r in range(len(sep_host.register_arrays)):
+        sep_host.register_arrays[r] = sep_host.register_arrays[r].pin_memory()
+    h2d = sum(a.numel() * 16 for a in sep_host.register_arrays)
+    nq = len(circ["qubits"]) - 1
+    d2h = nq * 2 * 8
+    sim = CudaCvdv(circ["qubits"], check_errors=True)
+    e2e_times = []
+    for it in range(args.warmup + max(2, min(args.steps, 5))):
+        torch.cuda.synchronize()
+        barrier(world)
+        t0 = time.perf_counter()
+        sim.initStateVector(sep_host)
+        W.apply(sim, circ["prep"])
+        W.apply(sim, circ["gates"])
+        probs = sim.mEach(list(range(nq)))
+        t1 = time.perf_counter()
+        if it >= args.warmup:
+            e2e_times.append(t1 - t0)
+    e2e_s = max_over_ranks(statistics.median(e2e_times), world)
+    del sim
+    torch.cuda.empty_cache()
+
+    # ---- mixed precision (complex64 state) on the same circuit
+    ms64, stats64, launches64, clocks64, norm64 = timed_run("complex64")
+    f64_ms, f64_n = stats64["fft_pass"]
+    pl64 = f64_ms / max(f64_n, 1)
+    ach64 = (2 * n_amp * 8 / passes) / (pl64 * 1e-3) / 1e9
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded circuit, seed 2)",
+        "config": {"workload": "state_transfer: registers [1]*14+[14], 2^28 amplitudes, 42 gates "
+                               "(14 x H, cd, Rz), complex128 state",
+                   "l2": "state 4 GiB > L2 126 MB, no flush needed", "parallelism": f"replicas x{world}"},
+        "amplitudes_per_s": value * n_amp,
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": "k_fft_pass (register FFT, 2 passes of radix 128)",
+                     "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "peak_kind": peak_kind, "traffic": None,
+                     "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": per_launch_ms,
+                     "launches": fft_n, "share_of_kernel_time": fft_ms / max(total_kernel_ms, 1e-12)},
+        "kernel_ms_per_step": {k: v[0] / args.steps for k, v in stats.items() if v[1]},
+        "clocks": clocks,
+        "e2e": {"value": G * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "includes": "init from host arrays + 2 prep gates + 42 gates + 14 marginals"},
+        "norm_after": norm,
+        "mixed_c64": {"value": G * world / (ms64 * 1e-3), "ms_per_step": ms64, "gpu_launches": int(launches64),
+                      "roofline_frac": ach64 / hbm, "achieved_gbs": ach64, "norm_after": norm64,
+                      "speedup_vs_plain": ms / ms64},
+    }
+    if world == 1 and rank == 0 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        times = cpu_oracle_gates(circ, [0, 1, 2], threads)
+        line["cpu_baseline"] = {"value": 3 / sum(times), "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": "round 1 (H, cd, Rz) of the circuit at full 2^28 size on the CPU oracle"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world, rank, local = dist_init()
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_gpu(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

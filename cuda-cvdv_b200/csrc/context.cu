@@ -1,0 +1,364 @@
+// Context lifecycle, error reporting, scratch memory, state I/O and the flush
+// planner.
+//
+// Reference interfaces replaced here: cvdvCreate / cvdvDestroy / cvdvFree /
+// cvdvInitFromSeparable / cvdvSetStateFromDevicePtr and the getters
+// (src/cuda/context.cu:7-163, declared in src/cuda/api.h:14-23).  Unlike the
+// reference, no entry point throws or exits: failures are recorded and can be
+// read back with cvdvGetLastError.
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <atomic>
+#include <map>
+#include <mutex>
+
+#include "cvdv_internal.cuh"
+
+namespace cvdv {
+
+static std::mutex g_errMu;
+static int g_lastErr = kOk;
+static std::string g_lastMsg;
+
+void set_error(Context* ctx, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (ctx) {
+    ctx->lastErr = code;
+    ctx->lastMsg = buf;
+  }
+  std::lock_guard<std::mutex> lk(g_errMu);
+  g_lastErr = code;
+  g_lastMsg = buf;
+  if (getenv("CVDV_VERBOSE")) fprintf(stderr, "cvdv error %d: %s\n", code, buf);
+}
+
+// ----------------------------------------------------------------- launch accounting
+std::atomic<unsigned long long> g_launches{0};
+static thread_local int t_scopeDepth = 0;
+static thread_local int t_scopeKind = 0;
+
+static cudaEvent_t pool_event(Context* c) {
+  if (!c->eventPool.empty()) {
+    cudaEvent_t e = c->eventPool.back();
+    c->eventPool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+void launch_begin(Context* c, int kind) {
+  if (t_scopeDepth++ > 0) return;  // nested scopes count once
+  t_scopeKind = kind;
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (c && c->timing) {
+    TimingRec r{pool_event(c), pool_event(c), kind};
+    cudaEventRecord(r.a, c->stream);
+    c->timingRecs.push_back(r);
+  }
+}
+
+void launch_end(Context* c) {
+  if (--t_scopeDepth > 0) return;
+  if (c && c->timing && !c->timingRecs.empty()) cudaEventRecord(c->timingRecs.back().b, c->stream);
+}
+
+void harvest_timing(Context* c) {
+  if (c->timingRecs.empty()) return;
+  cudaStreamSynchronize(c->stream);
+  for (auto& r : c->timingRecs) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+      c->kindMs[r.kind] += ms;
+      c->kindCount[r.kind] += 1;
+    } else {
+      cudaGetLastError();
+    }
+    c->eventPool.push_back(r.a);
+    c->eventPool.push_back(r.b);
+  }
+  c->timingRecs.clear();
+}
+
+int global_error(char* msg, int len) {
+  std::lock_guard<std::mutex> lk(g_errMu);
+  if (msg && len > 0) {
+    strncpy(msg, g_lastMsg.c_str(), (size_t)len - 1);
+    msg[len - 1] = 0;
+  }
+  return g_lastErr;
+}
+
+bool cuda_ok(Context* ctx, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return true;
+  set_error(ctx, kErrCuda, "%s: %s", what, cudaGetErrorString(e));
+  return false;
+}
+
+// ----------------------------------------------------------------- arena
+// Small per-flush scratch (factor tables, partial sums).  Allocation never
+// invalidates pointers handed out since the last reset: when the arena is full
+// a new block is chained; the next reset merges all blocks into one.
+void arena_reset(Context* ctx) {
+  if (!ctx->arenaExtra.empty()) {
+    size_t total = ctx->arenaCap;
+    for (auto& b : ctx->arenaExtra) total += b.cap;
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& b : ctx->arenaExtra) cudaFree(b.p);
+    ctx->arenaExtra.clear();
+    if (ctx->arena) cudaFree(ctx->arena);
+    ctx->arena = nullptr;
+    ctx->arenaCap = 0;
+    if (cudaMalloc(&ctx->arena, total) == cudaSuccess) ctx->arenaCap = total;
+    else cudaGetLastError();
+  }
+  ctx->arenaTop = 0;
+}
+
+void* arena_alloc(Context* ctx, size_t bytes) {
+  bytes = (bytes + 255) & ~(size_t)255;
+  if (ctx->arena && ctx->arenaTop + bytes <= ctx->arenaCap) {
+    void* p = ctx->arena + ctx->arenaTop;
+    ctx->arenaTop += bytes;
+    return p;
+  }
+  if (!ctx->arenaExtra.empty()) {
+    ArenaBlock& b = ctx->arenaExtra.back();
+    if (b.top + bytes <= b.cap) {
+      void* p = b.p + b.top;
+      b.top += bytes;
+      return p;
+    }
+  }
+  size_t cap = bytes < (64ull << 20) ? (64ull << 20) : bytes;
+  char* p = nullptr;
+  if (cudaMalloc(&p, cap) != cudaSuccess) {
+    cudaGetLastError();
+    set_error(ctx, kErrAlloc, "arena: cudaMalloc(%zu) failed", cap);
+    return nullptr;
+  }
+  ctx->arenaExtra.push_back({p, cap, bytes});
+  return p;
+}
+
+void* big_scratch(Context* ctx, size_t bytes) {
+  if (bytes <= ctx->bigCap) return ctx->big;
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->big) cudaFree(ctx->big);
+  ctx->big = nullptr;
+  ctx->bigCap = 0;
+  if (cudaMalloc(&ctx->big, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    set_error(ctx, kErrAlloc, "scratch: cudaMalloc(%zu) failed", bytes);
+    return nullptr;
+  }
+  ctx->bigCap = bytes;
+  return ctx->big;
+}
+
+double* host_scratch(Context* ctx, size_t count) {
+  size_t bytes = count * sizeof(double);
+  if (bytes <= ctx->hostScratchCap) return ctx->hostScratch;
+  if (ctx->hostScratch) cudaFreeHost(ctx->hostScratch);
+  ctx->hostScratch = nullptr;
+  ctx->hostScratchCap = 0;
+  if (cudaMallocHost(&ctx->hostScratch, bytes) != cudaSuccess) {
+    set_error(ctx, kErrAlloc, "pinned host scratch (%zu bytes) failed", bytes);
+    return nullptr;
+  }
+  ctx->hostScratchCap = bytes;
+  return ctx->hostScratch;
+}
+
+bool ensure_state(Context* ctx) {
+  if (ctx->numReg == 0) {
+    set_error(ctx, kErrNotInitialized, "context has no registers");
+    return false;
+  }
+  uint64_t n = ctx->size();
+  if (ctx->allocElems >= n && ctx->buf[0] && ctx->buf[1]) return true;
+  for (int k = 0; k < 2; ++k) {
+    if (ctx->buf[k]) cudaFree(ctx->buf[k]);
+    ctx->buf[k] = nullptr;
+  }
+  for (int k = 0; k < 2; ++k) {
+    if (cudaMalloc(&ctx->buf[k], n * ctx->elemBytes) != cudaSuccess) {
+      cudaGetLastError();
+      set_error(ctx, kErrAlloc, "state buffer %d: cudaMalloc(%llu bytes) failed", k,
+                (unsigned long long)(n * ctx->elemBytes));
+      if (ctx->buf[0]) cudaFree(ctx->buf[0]);
+      ctx->buf[0] = nullptr;
+      return false;
+    }
+  }
+  ctx->allocElems = n;
+  ctx->cur = 0;
+  return true;
+}
+
+// ----------------------------------------------------------------- factor lists
+struct TableKey {
+  int r;
+  int ctrl;  // external control bit or -1
+  bool operator<(const TableKey& o) const { return r != o.r ? r < o.r : ctrl < o.ctrl; }
+};
+
+static inline double2 hmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// Turn a diagonal run into a FactorList.  Terms that do not fit are returned in
+// `leftover` (diagonal terms commute, so they can run as a separate pass).
+bool build_factor_list(Context* ctx, const std::vector<Term>& terms, FactorList* F,
+                       std::vector<Term>* leftover) {
+  memset(F, 0, sizeof(*F));
+  F->scalar = make_double2(1.0, 0.0);
+  std::map<TableKey, std::vector<Term>> groups;
+  std::vector<const Term*> xx;
+  for (const Term& t : terms) {
+    if (t.kind == kTermScalar) {
+      F->scalar = hmul(F->scalar, t.g0);
+      F->hasScalar = 1;
+      continue;
+    }
+    if (t.kind == kTermXX) {
+      xx.push_back(&t);
+      continue;
+    }
+    int ctrl = -1;
+    if (t.kind == kTermPoly && t.ctrlBit >= 0) {
+      int lo = ctx->flw[t.r], hi = lo + ctx->q[t.r];
+      if (!(t.ctrlBit >= lo && t.ctrlBit < hi)) ctrl = t.ctrlBit;
+    }
+    groups[{t.r, ctrl}].push_back(t);
+  }
+  // fold each register's uncontrolled terms into one of its controlled tables
+  for (auto it = groups.begin(); it != groups.end();) {
+    if (it->first.ctrl == -1) {
+      auto jt = groups.end();
+      for (auto kt = groups.begin(); kt != groups.end(); ++kt)
+        if (kt->first.r == it->first.r && kt->first.ctrl >= 0) {
+          jt = kt;
+          break;
+        }
+      if (jt != groups.end() &&
+          jt->second.size() + it->second.size() <= (size_t)kMaxTermsPerTable) {
+        jt->second.insert(jt->second.end(), it->second.begin(), it->second.end());
+        it = groups.erase(it);
+        continue;
+      }
+    }
+    ++it;
+  }
+  for (auto& g : groups) {
+    const std::vector<Term>& ts = g.second;
+    for (size_t start = 0; start < ts.size(); start += kMaxTermsPerTable) {
+      size_t cnt = ts.size() - start;
+      if (cnt > (size_t)kMaxTermsPerTable) cnt = kMaxTermsPerTable;
+      if (F->nTab >= kMaxTab) {
+        leftover->insert(leftover->end(), ts.begin() + start, ts.begin() + start + cnt);
+        continue;
+      }
+      int r = g.first.r;
+      bool ctrl = g.first.ctrl >= 0;
+      int N = 1 << ctx->q[r];
+      double2* tab = (double2*)arena_alloc(ctx, (size_t)N * (ctrl ? 2 : 1) * sizeof(double2));
+      if (!tab) return false;
+      if (!launch_build_table(ctx, r, ctrl, ts.data() + start, (int)cnt, tab)) return false;
+      TabFactor& T = F->tab[F->nTab++];
+      T.ptr = tab;
+      T.shift = ctx->flw[r];
+      T.mask = N - 1;
+      T.ctrlShift = ctrl ? g.first.ctrl : -1;
+      T.half = N;
+    }
+  }
+  for (const Term* t : xx) {
+    if (F->nXX >= kMaxXX) {
+      leftover->push_back(*t);
+      continue;
+    }
+    XXFactor& X = F->xx[F->nXX++];
+    X.shift1 = ctx->flw[t->r];
+    X.mask1 = (1 << ctx->q[t->r]) - 1;
+    X.shift2 = ctx->flw[t->s];
+    X.mask2 = (1 << ctx->q[t->s]) - 1;
+    X.c1 = (double)((1 << ctx->q[t->r]) - 1) * 0.5;
+    X.dx1 = ctx->dx[t->r];
+    X.c2 = (double)((1 << ctx->q[t->s]) - 1) * 0.5;
+    X.dx2 = ctx->dx[t->s];
+    X.coeff = t->coeff;
+    X.ctrlShift = t->ctrlBit;
+  }
+  return true;
+}
+
+static bool run_leftover(Context* ctx, std::vector<Term> terms) {
+  while (!terms.empty()) {
+    FactorList F;
+    std::vector<Term> rest;
+    if (!build_factor_list(ctx, terms, &F, &rest)) return false;
+    if (!factor_empty(F) && !launch_diag(ctx, F)) return false;
+    if (rest.size() == terms.size()) {
+      set_error(ctx, kErrUnsupported, "diagonal run could not be planned");
+      return false;
+    }
+    terms.swap(rest);
+  }
+  return true;
+}
+
+// ----------------------------------------------------------------- flush
+struct Op {
+  const Stage* st;
+  std::vector<Term> pre, post;
+};
+
+bool flush(Context* ctx) {
+  if (ctx->pending.empty()) return true;
+  if (!ctx->initialized) {
+    set_error(ctx, kErrNotInitialized, "gates queued before the state was initialised");
+    ctx->pending.clear();
+    return false;
+  }
+  arena_reset(ctx);
+  std::vector<Stage> stages;
+  stages.swap(ctx->pending);
+  std::vector<Op> ops;
+  std::vector<Term> diag;
+  for (const Stage& s : stages) {
+    if (s.kind == kStDiag) {
+      diag.insert(diag.end(), s.terms.begin(), s.terms.end());
+      continue;
+    }
+    ops.push_back({&s, diag, {}});
+    diag.clear();
+  }
+  if (ops.empty()) return run_leftover(ctx, diag);
+  ops.back().post = diag;
+  for (Op& op : ops) {
+    FactorList pre, post;
+    std::vector<Term> lpre, lpost;
+    if (!build_factor_list(ctx, op.pre, &pre, &lpre)) return false;
+    if (!build_factor_list(ctx, op.post, &post, &lpost)) return false;
+    if (!run_leftover(ctx, lpre)) return false;
+    const Stage& s = *op.st;
+    bool ok = true;
+    if (s.kind == kStFft) ok = launch_fft(ctx, s.reg, s.dir, pre, post);
+    else if (s.kind == kStPair) ok = launch_pair(ctx, s.bit, s.m, pre, post);
+    else if (s.kind == kStPerm) ok = launch_perm(ctx, s, pre, post);
+    if (!ok) return false;
+    if (!run_leftover(ctx, lpost)) return false;
+  }
+  return true;
+}
+
+}  // namespace cvdv

@@ -1,0 +1,453 @@
+// Phase-space readouts: Wigner and Husimi-Q of one register, other registers
+// traced out.
+//
+// Wigner (reference: cvdvGetWigner, src/cuda/bosonic.cu:103-132 with kernels
+// src/cuda/kernels/bosonic.cuh:7-52).  The reference builds
+//   G[i,k] = sum_o conj(psi_o[i+kd]) psi_o[i-kd],  kd = k - (N-1)/2,
+// with one thread per (i,k) looping over all M other-register slices through
+// uncoalesced gathers, O(N^2 M).  Here the same sum is read off the reduced
+// density matrix rho[a][b] = sum_o psi_o[a] conj(psi_o[b]), formed as a tiled
+// Hermitian GEMM (upper-triangle tiles only, FP64 accumulation, shared-memory
+// operand tiles), then G[i,k] = rho[i-kd][i+kd] is gathered, a batched inverse
+// FFT runs along k, and a transposing epilogue applies the phase correction,
+// the fftshift and dx/pi.
+//
+// Husimi-Q (reference: husimiFromOverlap, bosonic.cu:10-61 and
+// husimiFromWignerFft2, bosonic.cu:63-101) follows the same two routes and the
+// same memory rule for choosing between them.
+
+#include <cmath>
+#include <cstring>
+
+#include "../../include/cvdv.h"
+#include "cvdv_internal.cuh"
+
+using namespace cvdv;
+struct CVDVContext : public cvdv::Context {};
+
+namespace cvdv {
+
+template <typename C> __device__ __forceinline__ double2 tod2(C v);
+template <> __device__ __forceinline__ double2 tod2<double2>(double2 v) { return v; }
+template <> __device__ __forceinline__ double2 tod2<float2>(float2 v) {
+  return make_double2((double)v.x, (double)v.y);
+}
+
+// psi_o[a]: slice o of register r (low bits below the register, then high bits),
+// local index a -- the ordering of kernelExtractChunkPsi (bosonic.cuh:93-106).
+__device__ __forceinline__ uint64_t slice_addr(uint64_t o, uint64_t a, int flw, int q) {
+  uint64_t lowMask = (1ull << flw) - 1;
+  return ((o & ~lowMask) << q) | (a << flw) | (o & lowMask);
+}
+
+// ----------------------------------------------------------------- rho GEMM
+constexpr int kRT = 64;   // output tile
+constexpr int kRK = 16;   // slices per k-step
+
+template <typename C>
+__global__ void __launch_bounds__(256) k_rho(const C* __restrict__ st, int N, int q, int flw,
+                                            uint64_t M, double2* __restrict__ rho, int aFast) {
+  int ta = blockIdx.y, tb = blockIdx.x;
+  if (ta > tb) return;  // Hermitian: upper tiles only
+  __shared__ double2 sA[kRK][kRT + 1];
+  __shared__ double2 sB[kRK][kRT + 1];
+  const int a0 = ta * kRT, b0 = tb * kRT;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double2 acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = make_double2(0.0, 0.0);
+  for (uint64_t o0 = 0; o0 < M; o0 += kRK) {
+    for (int e = threadIdx.x; e < kRK * kRT; e += 256) {
+      int kk, a;
+      if (aFast) {
+        a = e % kRT;
+        kk = e / kRT;
+      } else {
+        kk = e % kRK;
+        a = e / kRK;
+      }
+      uint64_t o = o0 + kk;
+      double2 va = make_double2(0.0, 0.0), vb = make_double2(0.0, 0.0);
+      if (o < M) {
+        if (a0 + a < N) va = tod2<C>(st[slice_addr(o, a0 + a, flw, q)]);
+        if (b0 + a < N) vb = tod2<C>(st[slice_addr(o, b0 + a, flw, q)]);
+      }
+      sA[kk][a] = va;
+      sB[kk][a] = vb;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < kRK; ++kk) {
+      double2 av[4], bv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) av[i] = sA[kk][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bv[j] = sB[kk][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          // a * conj(b)
+          acc[i][j].x += av[i].x * bv[j].x + av[i].y * bv[j].y;
+          acc[i][j].y += av[i].y * bv[j].x - av[i].x * bv[j].y;
+        }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int a = a0 + ty + 16 * i, b = b0 + tx + 16 * j;
+      if (a < N && b < N) rho[(size_t)a * N + b] = acc[i][j];
+    }
+}
+
+// G[i][k] = rho[i-kd][i+kd] (conj-symmetric lookup), 0 off the grid
+__global__ void k_wigner_gather(const double2* __restrict__ rho, int N, double2* __restrict__ G) {
+  uint64_t NN = (uint64_t)N * N;
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < NN;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    int i = (int)(e / N), k = (int)(e % N);
+    int kd = k - (N - 1) / 2;
+    int ip = i + kd, im = i - kd;
+    double2 v = make_double2(0.0, 0.0);
+    if (ip >= 0 && ip < N && im >= 0 && im < N) {
+      if (im <= ip) {
+        v = rho[(size_t)im * N + ip];
+      } else {
+        v = rho[(size_t)ip * N + im];
+        v.y = -v.y;
+      }
+    }
+    G[e] = v;
+  }
+}
+
+// W[jc][i] = Re(H[i][(jc+N/2)%N] e^{i phi_jc}) dx/pi, phi_jc = -pi (jc-N/2)(N-1)/N
+// (kernelFinalizeWigner, bosonic.cuh:39-52; phase reduced exactly).
+// Writes real (complexOut == nullptr) or complex (w, 0) output.
+__global__ void k_wigner_finalize(const double2* __restrict__ H, int N, double dx,
+                                  double* __restrict__ out, double2* __restrict__ complexOut) {
+  __shared__ double tile[32][33];
+  int jc0 = blockIdx.x * 32, i0 = blockIdx.y * 32;
+  int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  for (int r = ty; r < 32; r += 8) {
+    int i = i0 + r, jc = jc0 + tx;
+    if (i < N && jc < N) {
+      int kf = (jc + N / 2) % N;
+      double2 g = H[(size_t)i * N + kf];
+      long long m = -(long long)(jc - N / 2) * (long long)(N - 1);
+      long long M2 = 2LL * N;
+      m %= M2;
+      if (m < 0) m += M2;
+      double s, c;
+      sincospi((double)m / (double)N, &s, &c);
+      tile[r][tx] = (g.x * c - g.y * s) * dx / CVDV_PI;
+    }
+  }
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8) {
+    int jc = jc0 + r, i = i0 + tx;
+    if (i < N && jc < N) {
+      double w = tile[tx][r];
+      if (complexOut) complexOut[(size_t)jc * N + i] = make_double2(w, 0.0);
+      else out[(size_t)jc * N + i] = w;
+    }
+  }
+}
+
+// ----------------------------------------------------------------- Husimi kernels
+template <typename C>
+__global__ void k_extract_slices(const C* __restrict__ st, int N, int q, int flw, uint64_t s0,
+                                 uint64_t cnt, double2* __restrict__ X) {
+  uint64_t tot = cnt * (uint64_t)N;
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t s = e / N, x = e % N;
+    X[e] = tod2<C>(st[slice_addr(s0 + s, x, flw, q)]);
+  }
+}
+
+// G[k] = pi^{1/4} sqrt(2/dx) exp(-p^2/2), p = 2 pi k_signed / (N dx)  (bosonic.cuh:82-89)
+__device__ __forceinline__ double husimi_g(int k, int N, double dx) {
+  int ks = (k <= N / 2) ? k : k - N;
+  double p = 2.0 * CVDV_PI * ks / ((double)N * dx);
+  return pow(CVDV_PI, 0.25) * sqrt(2.0 / dx) * exp(-0.5 * p * p);
+}
+
+// A[s][m][k] = Psi_s[(m+k) & (N-1)] G[k]   (kernelFillHusimiABatched, bosonic.cuh:112-125)
+__global__ void k_husimi_fill(const double2* __restrict__ Psi, int N, double dx, uint64_t cnt,
+                              double2* __restrict__ A) {
+  uint64_t NN = (uint64_t)N * N, tot = cnt * NN;
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t s = e / NN;
+    uint64_t rem = e % NN;
+    int m = (int)(rem / N), k = (int)(rem % N);
+    double2 p = Psi[s * N + ((m + k) & (N - 1))];
+    double g = husimi_g(k, N, dx);
+    A[e] = make_double2(p.x * g, p.y * g);
+  }
+}
+
+// acc[m][j] += sum_s |H[s][m][j]|^2   (kernelAccumHusimiPowerChunked, bosonic.cuh:142-150)
+__global__ void k_husimi_accum(const double2* __restrict__ H, uint64_t NN, uint64_t cnt,
+                               double* __restrict__ acc) {
+  for (uint64_t pos = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; pos < NN;
+       pos += (uint64_t)gridDim.x * blockDim.x) {
+    double a = 0.0;
+    for (uint64_t s = 0; s < cnt; ++s) {
+      double2 v = H[s * NN + pos];
+      a += v.x * v.x + v.y * v.y;
+    }
+    acc[pos] += a;
+  }
+}
+
+// Q[jc][q] = acc[(jc+N/2)%N][q] / (pi N^2)   (kernelFinalizeHusimi, bosonic.cuh:128-138)
+__global__ void k_husimi_finalize(const double* __restrict__ acc, int N, double* __restrict__ out) {
+  uint64_t NN = (uint64_t)N * N;
+  double norm = CVDV_PI * (double)N * (double)N;
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < NN;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    int jc = (int)(e / N), qq = (int)(e % N);
+    int m = (jc + N / 2) % N;
+    out[e] = acc[(size_t)m * N + qq] / norm;
+  }
+}
+
+// x exp(-(wq^2 + wp^2)/4) in 2-D frequency space (kernelApplyHusimiGaussian2DFreq,
+// bosonic.cuh:158-177)
+__global__ void k_husimi_gauss2d(double2* __restrict__ spec, int N, double dx) {
+  uint64_t NN = (uint64_t)N * N;
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < NN;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    int p = (int)(e / N), qq = (int)(e % N);
+    int kq = (qq <= N / 2) ? qq : qq - N;
+    int kp = (p <= N / 2) ? p : p - N;
+    double Lq = (double)N * dx;
+    double dp = CVDV_PI / ((double)N * dx);
+    double Lp = (double)N * dp;
+    double wq = 2.0 * CVDV_PI * (double)kq / Lq;
+    double wp = 2.0 * CVDV_PI * (double)kp / Lp;
+    double g = exp(-0.25 * (wq * wq + wp * wp));
+    spec[e] = make_double2(spec[e].x * g, spec[e].y * g);
+  }
+}
+
+// max(Re / N^2, 0)   (kernelComplexToRealNormalizedClamp, bosonic.cuh:180-186)
+__global__ void k_real_clamp(const double2* __restrict__ in, uint64_t NN, double norm,
+                             double* __restrict__ out) {
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < NN;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    double v = in[e].x / norm;
+    out[e] = v < 0.0 ? 0.0 : v;
+  }
+}
+
+static int gblocks(uint64_t work) {
+  uint64_t b = (work + 255) / 256;
+  return (int)(b < 148 * 16 ? (b < 1 ? 1 : b) : 148 * 16);
+}
+
+// Wigner into device memory: real W (out) or complex (w, 0) (complexOut).
+// Scratch layout in big: [rho | G/H | tmp] each N^2 complex.
+static bool wigner_device(Context* c, int r, double* out, double2* complexOut, double2* work) {
+  int q = c->q[r], flw = c->flw[r];
+  int N = 1 << q;
+  uint64_t M = c->size() >> q;
+  size_t NN = (size_t)N * N;
+  double2* rho = work;
+  double2* G = work + NN;
+  double2* T = work + 2 * NN;
+  dim3 g((N + kRT - 1) / kRT, (N + kRT - 1) / kRT);
+  int aFast = flw == 0 ? 1 : 0;
+  if (c->precision == kC128)
+    {
+      LaunchScope _ls(c, kKPhaseSpace);
+      k_rho<double2><<<g, 256, 0, c->stream>>>((const double2*)c->state(), N, q, flw, M, rho, aFast);
+    }
+  else
+    {
+      LaunchScope _ls(c, kKPhaseSpace);
+      k_rho<float2><<<g, 256, 0, c->stream>>>((const float2*)c->state(), N, q, flw, M, rho, aFast);
+    }
+  {
+    LaunchScope _ls(c, kKPhaseSpace);
+    k_wigner_gather<<<gblocks(NN), 256, 0, c->stream>>>(rho, N, G);
+  }
+  if (!cuda_ok(c, cudaGetLastError(), "wigner launch")) return false;
+  // inverse FFT along k (rows contiguous); the result lands in rho's buffer
+  if (!launch_fft_generic(c, G, rho, T, (uint64_t)N, q, 1, -1, kC128)) {
+    set_error(c, kErrUnsupported, "wigner: register too large for the row FFT");
+    return false;
+  }
+  dim3 fg((N + 31) / 32, (N + 31) / 32);
+  {
+    LaunchScope _ls(c, kKPhaseSpace);
+    k_wigner_finalize<<<fg, dim3(32, 8), 0, c->stream>>>(rho, N, c->dx[r], out, complexOut);
+  }
+  return cuda_ok(c, cudaGetLastError(), "wigner finalize");
+}
+
+}  // namespace cvdv
+
+static Context* C(CVDVContext* p) { return static_cast<Context*>(p); }
+
+static bool prep(Context* c, int regIdx, void* out, const char* w) {
+  if (regIdx < 0 || regIdx >= c->numReg || !out) {
+    set_error(c, kErrInvalidArg, "%s: invalid register index %d", w, regIdx);
+    return false;
+  }
+  if (c->numReg == 0 || !c->initialized) {
+    set_error(c, kErrNotInitialized, "%s: state not initialised", w);
+    return false;
+  }
+  return flush(c);
+}
+
+static void husimi_wigner_route(Context* c, int r, double* husimiOut) {
+  int q = c->q[r];
+  int N = 1 << q;
+  size_t NN = (size_t)N * N;
+  double2* work = (double2*)big_scratch(c, 4 * NN * sizeof(double2));
+  if (!work) return;
+  double2* Wc = work + 3 * NN;
+  if (!wigner_device(c, r, nullptr, Wc, work)) return;
+  double2* A = work;
+  double2* B = work + NN;
+  // 2-D FFT: along q (contiguous rows), then along p (stride N)
+  if (!launch_fft_generic(c, Wc, A, B, (uint64_t)N, q, 1, 1, kC128) ||
+      !launch_fft_generic(c, A, Wc, B, 1, q, (uint64_t)N, 1, kC128)) {
+    set_error(c, kErrUnsupported, "husimi: register too large");
+    return;
+  }
+  {
+    LaunchScope _ls(c, kKPhaseSpace);
+    k_husimi_gauss2d<<<gblocks(NN), 256, 0, c->stream>>>(Wc, N, c->dx[r]);
+  }
+  if (!launch_fft_generic(c, Wc, A, B, (uint64_t)N, q, 1, -1, kC128) ||
+      !launch_fft_generic(c, A, Wc, B, 1, q, (uint64_t)N, -1, kC128))
+    return;
+  double* dOut = (double*)B;
+  {
+    LaunchScope _ls(c, kKPhaseSpace);
+    k_real_clamp<<<gblocks(NN), 256, 0, c->stream>>>(Wc, NN, (double)NN, dOut);
+  }
+  if (!cuda_ok(c, cudaMemcpyAsync(husimiOut, dOut, NN * sizeof(double), cudaMemcpyDeviceToHost,
+                                  c->stream), "husimi copy"))
+    return;
+  cuda_ok(c, cudaStreamSynchronize(c->stream), "husimi sync");
+}
+
+static void husimi_overlap_route(Context* c, int r, double* husimiOut) {
+  int q = c->q[r], flw = c->flw[r];
+  int N = 1 << q;
+  uint64_t S = c->size() >> q;
+  size_t NN = (size_t)N * N;
+  // slices per chunk: the circulant A of a chunk holds cs * N^2 complex values
+  uint64_t cs = ((uint64_t)1 << 25) / NN;
+  if (cs < 1) cs = 1;
+  if (cs > S) cs = S;
+  size_t need = (size_t)(2 * S * N + 3 * cs * NN) * sizeof(double2) + NN * sizeof(double);
+  char* work = (char*)big_scratch(c, need);
+  if (!work) return;
+  double2* X = (double2*)work;
+  double2* Psi = X + S * N;
+  double2* A = Psi + S * N;
+  double2* H = A + cs * NN;
+  double2* T = H + cs * NN;  // temporary of a two-pass row transform
+  double* acc = (double*)(T + cs * NN);
+  if (c->precision == kC128)
+    {
+      LaunchScope _ls(c, kKPhaseSpace);
+      k_extract_slices<double2><<<gblocks(S * N), 256, 0, c->stream>>>((const double2*)c->state(), N, q, flw, 0, S, X);
+    }
+  else
+    {
+      LaunchScope _ls(c, kKPhaseSpace);
+      k_extract_slices<float2><<<gblocks(S * N), 256, 0, c->stream>>>((const float2*)c->state(), N, q, flw, 0, S, X);
+    }
+  if (!launch_fft_generic(c, X, Psi, A, S, q, 1, 1, kC128)) {
+    set_error(c, kErrUnsupported, "husimi: register too large");
+    return;
+  }
+  cudaMemsetAsync(acc, 0, NN * sizeof(double), c->stream);
+  for (uint64_t s0 = 0; s0 < S; s0 += cs) {
+    uint64_t cnt = S - s0 < cs ? S - s0 : cs;
+    {
+      LaunchScope _ls(c, kKPhaseSpace);
+      k_husimi_fill<<<gblocks(cnt * NN), 256, 0, c->stream>>>(Psi + s0 * N, N, c->dx[r], cnt, A);
+    }
+    // inverse FFT of every (s, m) row
+    if (!launch_fft_generic(c, A, H, T, cnt * N, q, 1, -1, kC128)) return;
+    {
+      LaunchScope _ls(c, kKPhaseSpace);
+      k_husimi_accum<<<gblocks(NN), 256, 0, c->stream>>>(H, NN, cnt, acc);
+    }
+  }
+  double* dOut = (double*)A;
+  {
+    LaunchScope _ls(c, kKPhaseSpace);
+    k_husimi_finalize<<<gblocks(NN), 256, 0, c->stream>>>(acc, N, dOut);
+  }
+  if (!cuda_ok(c, cudaGetLastError(), "husimi launch")) return;
+  if (!cuda_ok(c, cudaMemcpyAsync(husimiOut, dOut, NN * sizeof(double), cudaMemcpyDeviceToHost,
+                                  c->stream), "husimi copy"))
+    return;
+  cuda_ok(c, cudaStreamSynchronize(c->stream), "husimi sync");
+}
+
+// The reference chooses the Wigner route when the overlap route's buffers would
+// exceed 80% of free device memory (bosonic.cu:14-25); the same rule applies.
+static bool overlap_fits(Context* c, int r) {
+  size_t N = (size_t)1 << c->q[r];
+  size_t S = (size_t)(c->size() >> c->q[r]);
+  size_t fixedBytes = N * 16 + 2 * N * N * 8;
+  double dyn = (double)S * N * 16 + (double)S * N * N * 16;
+  size_t freeB = 0, totalB = 0;
+  if (cudaMemGetInfo(&freeB, &totalB) != cudaSuccess) return false;
+  return (double)fixedBytes + dyn <= 0.8 * (double)freeB;
+}
+
+extern "C" {
+
+void cvdvGetWigner(CVDVContext* ctx, int regIdx, double* wignerOut) {
+  if (!ctx) return;
+  Context* c = C(ctx);
+  if (!prep(c, regIdx, wignerOut, "cvdvGetWigner")) return;
+  int N = 1 << c->q[regIdx];
+  size_t NN = (size_t)N * N;
+  double2* work = (double2*)big_scratch(c, 3 * NN * sizeof(double2) + NN * sizeof(double));
+  if (!work) return;
+  double* dOut = (double*)(work + 3 * NN);
+  if (!wigner_device(c, regIdx, dOut, nullptr, work)) return;
+  if (!cuda_ok(c, cudaMemcpyAsync(wignerOut, dOut, NN * sizeof(double), cudaMemcpyDeviceToHost,
+                                  c->stream), "wigner copy"))
+    return;
+  cuda_ok(c, cudaStreamSynchronize(c->stream), "wigner sync");
+}
+
+void cvdvGetHusimiQ(CVDVContext* ctx, int regIdx, double* husimiOut) {
+  if (!ctx) return;
+  Context* c = C(ctx);
+  if (!prep(c, regIdx, husimiOut, "cvdvGetHusimiQ")) return;
+  if (overlap_fits(c, regIdx)) husimi_overlap_route(c, regIdx, husimiOut);
+  else husimi_wigner_route(c, regIdx, husimiOut);
+}
+
+void cvdvGetHusimiQOverlap(CVDVContext* ctx, int regIdx, double* husimiOut) {
+  cvdvGetHusimiQ(ctx, regIdx, husimiOut);  // bosonic.cu:140-144 has the same fallback
+}
+
+void cvdvGetHusimiQWigner(CVDVContext* ctx, int regIdx, double* husimiOut) {
+  if (!ctx) return;
+  Context* c = C(ctx);
+  if (!prep(c, regIdx, husimiOut, "cvdvGetHusimiQWigner")) return;
+  husimi_wigner_route(c, regIdx, husimiOut);
+}
+
+}  // extern "C"

@@ -1,0 +1,547 @@
+// Readouts: state I/O, norm, fidelities, marginals and <n>.
+//
+// Reductions are two-level and deterministic where they produce a scalar: a
+// fixed grid writes one partial per block, a single block sums the partials in
+// a fixed order.  Marginals accumulate per-block shared-memory histograms with
+// warp aggregation (one shared atomic per warp when every lane of the warp
+// falls in the same bin, which is the case whenever the selected registers are
+// not the lowest 5 index bits), then sum the per-block histograms bin by bin.
+
+#include <cmath>
+#include <cstring>
+
+#include "../../include/cvdv.h"
+#include "cvdv_internal.cuh"
+
+using namespace cvdv;
+struct CVDVContext : public cvdv::Context {};
+
+namespace cvdv {
+
+constexpr int kRedBlocks = 148 * 4;
+constexpr int kRedThreads = 256;
+
+template <typename C> __device__ __forceinline__ double2 tod(C v);
+template <> __device__ __forceinline__ double2 tod<double2>(double2 v) { return v; }
+template <> __device__ __forceinline__ double2 tod<float2>(float2 v) {
+  return make_double2((double)v.x, (double)v.y);
+}
+
+__device__ __forceinline__ double2 block_sum2(double2 v) {
+  __shared__ double2 ws[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v.x += __shfl_down_sync(0xffffffffu, v.x, o);
+    v.y += __shfl_down_sync(0xffffffffu, v.y, o);
+  }
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) ws[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = lane < (int)(blockDim.x >> 5) ? ws[lane] : make_double2(0.0, 0.0);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      v.x += __shfl_down_sync(0xffffffffu, v.x, o);
+      v.y += __shfl_down_sync(0xffffffffu, v.y, o);
+    }
+  }
+  return v;
+}
+
+__global__ void k_final_sum(const double2* __restrict__ part, int n, double2* out) {
+  double2 a = make_double2(0.0, 0.0);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    a.x += part[i].x;
+    a.y += part[i].y;
+  }
+  a = block_sum2(a);
+  if (threadIdx.x == 0) *out = a;
+}
+
+// ---- functors for the generic reduction: return a double2 per index
+template <typename C>
+struct OpNorm {  // sum |psi|^2    (measure.cu:276-300)
+  const C* st;
+  __device__ double2 operator()(uint64_t i) const {
+    double2 v = tod<C>(st[i]);
+    return make_double2(v.x * v.x + v.y * v.y, 0.0);
+  }
+};
+
+template <typename C>
+struct OpX2 {  // sum |psi|^2 x_j^2   (kernelExpectX2, measure.cuh:158-178)
+  const C* st;
+  int shift, mask;
+  double c, dx;
+  __device__ double2 operator()(uint64_t i) const {
+    double2 v = tod<C>(st[i]);
+    double x = ((double)((i >> shift) & (uint64_t)mask) - c) * dx;
+    return make_double2((v.x * v.x + v.y * v.y) * x * x, 0.0);
+  }
+};
+
+template <typename C1, typename C2>
+struct OpDot {  // sum conj(a) b   (kernelInnerProductStatevectors, measure.cuh:227-252)
+  const C1* a;
+  const C2* b;
+  __device__ double2 operator()(uint64_t i) const {
+    double2 x = tod<C1>(a[i]), y = tod<C2>(b[i]);
+    return make_double2(x.x * y.x + x.y * y.y, x.x * y.y - x.y * y.x);
+  }
+};
+
+template <typename C>
+struct OpSep {  // sum conj(psi) * outer[i >> qLast] * last[i & m]   (measure.cuh:182-223)
+  const C* st;
+  const double2* outer;
+  const double2* last;
+  int qLast;
+  __device__ double2 operator()(uint64_t i) const {
+    double2 v = tod<C>(st[i]);
+    double2 p = dmul(__ldg(last + (i & ((1ull << qLast) - 1))), __ldg(outer + (i >> qLast)));
+    return make_double2(v.x * p.x + v.y * p.y, v.x * p.y - v.y * p.x);
+  }
+};
+
+template <typename Op>
+__global__ void __launch_bounds__(kRedThreads) k_reduce(Op op, uint64_t n, double2* part) {
+  double2 a = make_double2(0.0, 0.0);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    double2 v = op(i);
+    a.x += v.x;
+    a.y += v.y;
+  }
+  a = block_sum2(a);
+  if (threadIdx.x == 0) part[blockIdx.x] = a;
+}
+
+template <typename Op>
+static bool reduce(Context* ctx, Op op, uint64_t n, double2* result) {
+  double2* part = (double2*)arena_alloc(ctx, (kRedBlocks + 1) * sizeof(double2));
+  if (!part) return false;
+  double* hs = host_scratch(ctx, 2);
+  if (!hs) return false;
+  {
+    LaunchScope _ls(ctx, kKReduce);
+    k_reduce<Op><<<kRedBlocks, kRedThreads, 0, ctx->stream>>>(op, n, part);
+  }
+  {
+    LaunchScope _ls(ctx, kKReduce);
+    k_final_sum<<<1, 1024, 0, ctx->stream>>>(part, kRedBlocks, part + kRedBlocks);
+  }
+  if (!cuda_ok(ctx, cudaGetLastError(), "reduce launch")) return false;
+  if (!cuda_ok(ctx, cudaMemcpyAsync(hs, part + kRedBlocks, sizeof(double2), cudaMemcpyDeviceToHost,
+                                    ctx->stream),
+               "reduce copy"))
+    return false;
+  if (!cuda_ok(ctx, cudaStreamSynchronize(ctx->stream), "reduce sync")) return false;
+  *result = make_double2(hs[0], hs[1]);
+  return true;
+}
+
+// ----------------------------------------------------------------- marginals
+struct MargDesc {
+  int nSel;
+  int shift[16];
+  int mask[16];
+  long long stride[16];
+  long long outSize;
+};
+
+__device__ __forceinline__ long long marg_bin(const MargDesc& D, uint64_t i) {
+  long long oi = 0;
+  for (int s = 0; s < D.nSel; ++s) oi += (long long)((i >> D.shift[s]) & (uint64_t)D.mask[s]) * D.stride[s];
+  return oi;
+}
+
+// smem histogram per block -> part[block][bin]
+template <typename C>
+__global__ void __launch_bounds__(256) k_marg_smem(const C* __restrict__ st, uint64_t n,
+                                                  MargDesc D, double* __restrict__ part) {
+  extern __shared__ double hist[];
+  for (int b = threadIdx.x; b < D.outSize; b += blockDim.x) hist[b] = 0.0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const uint64_t warpStride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n;
+       base += warpStride) {
+    uint64_t i = base + lane;
+    double p = 0.0;
+    long long bin = 0;
+    if (i < n) {
+      double2 v = tod<C>(st[i]);
+      p = v.x * v.x + v.y * v.y;
+      bin = marg_bin(D, i);
+    }
+    long long b0 = __shfl_sync(0xffffffffu, bin, 0);
+    bool same = __all_sync(0xffffffffu, (i >= n) || bin == b0);
+    if (same) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) p += __shfl_down_sync(0xffffffffu, p, o);
+      if (lane == 0) atomicAdd(&hist[b0], p);
+    } else if (i < n) {
+      atomicAdd(&hist[bin], p);
+    }
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < D.outSize; b += blockDim.x)
+    part[(size_t)blockIdx.x * D.outSize + b] = hist[b];
+}
+
+__global__ void k_marg_final(const double* __restrict__ part, int nb, long long outSize,
+                             double* __restrict__ out) {
+  for (long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x; b < outSize;
+       b += (long long)gridDim.x * blockDim.x) {
+    double a = 0.0;
+    for (int k = 0; k < nb; ++k) a += part[(size_t)k * outSize + b];
+    out[b] = a;
+  }
+}
+
+// large outputs: global atomics (warp-aggregated when the warp shares a bin)
+template <typename C>
+__global__ void __launch_bounds__(256) k_marg_global(const C* __restrict__ st, uint64_t n,
+                                                    MargDesc D, double* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warpStride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n;
+       base += warpStride) {
+    uint64_t i = base + lane;
+    double p = 0.0;
+    long long bin = 0;
+    if (i < n) {
+      double2 v = tod<C>(st[i]);
+      p = v.x * v.x + v.y * v.y;
+      bin = marg_bin(D, i);
+    }
+    long long b0 = __shfl_sync(0xffffffffu, bin, 0);
+    bool same = __all_sync(0xffffffffu, (i >= n) || bin == b0);
+    if (same) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) p += __shfl_down_sync(0xffffffffu, p, o);
+      if (lane == 0) atomicAdd(&out[b0], p);
+    } else if (i < n) {
+      atomicAdd(&out[bin], p);
+    }
+  }
+}
+
+static bool marginal_device(Context* ctx, const int* regs, int nr, double** dOut, long long* outSize) {
+  MargDesc D{};
+  D.nSel = nr;
+  long long stride = 1;
+  for (int s = 0; s < nr; ++s) {
+    D.shift[s] = ctx->flw[regs[s]];
+    D.mask[s] = (1 << ctx->q[regs[s]]) - 1;
+    D.stride[s] = stride;  // column-major: first selected register fastest (measure.cu:89-91)
+    stride *= (long long)1 << ctx->q[regs[s]];
+  }
+  D.outSize = stride;
+  *outSize = stride;
+  uint64_t n = ctx->size();
+  double* out = (double*)arena_alloc(ctx, (size_t)stride * sizeof(double));
+  if (!out) return false;
+  if (stride <= 4096) {
+    int blocks = 148 * 2;
+    uint64_t maxBlocks = (n + 255) / 256;
+    if ((uint64_t)blocks > maxBlocks) blocks = (int)maxBlocks;
+    double* part = (double*)arena_alloc(ctx, (size_t)blocks * stride * sizeof(double));
+    if (!part) return false;
+    size_t smem = (size_t)stride * sizeof(double);
+    if (ctx->precision == kC128)
+      {
+        LaunchScope _ls(ctx, kKReduce);
+        k_marg_smem<double2><<<blocks, 256, smem, ctx->stream>>>((const double2*)ctx->state(), n, D, part);
+      }
+    else
+      {
+        LaunchScope _ls(ctx, kKReduce);
+        k_marg_smem<float2><<<blocks, 256, smem, ctx->stream>>>((const float2*)ctx->state(), n, D, part);
+      }
+    int fb = (int)((stride + 255) / 256);
+    {
+      LaunchScope _ls(ctx, kKReduce);
+      k_marg_final<<<fb, 256, 0, ctx->stream>>>(part, blocks, stride, out);
+    }
+  } else {
+    if (!cuda_ok(ctx, cudaMemsetAsync(out, 0, (size_t)stride * sizeof(double), ctx->stream), "memset"))
+      return false;
+    int blocks = 148 * 8;
+    if (ctx->precision == kC128)
+      {
+        LaunchScope _ls(ctx, kKReduce);
+        k_marg_global<double2><<<blocks, 256, 0, ctx->stream>>>((const double2*)ctx->state(), n, D, out);
+      }
+    else
+      {
+        LaunchScope _ls(ctx, kKReduce);
+        k_marg_global<float2><<<blocks, 256, 0, ctx->stream>>>((const float2*)ctx->state(), n, D, out);
+      }
+  }
+  if (!cuda_ok(ctx, cudaGetLastError(), "marginal launch")) return false;
+  *dOut = out;
+  return true;
+}
+
+// ----------------------------------------------------------------- conversions
+__global__ void k_c128_to_c64(const double2* __restrict__ s, float2* __restrict__ d, uint64_t n) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    d[i] = make_float2((float)s[i].x, (float)s[i].y);
+}
+
+bool launch_convert_c128_to_c64(Context* ctx, const double2* src, float2* dst, uint64_t n) {
+  {
+    LaunchScope _ls(ctx, kKInit);
+    k_c128_to_c64<<<148 * 8, 256, 0, ctx->stream>>>(src, dst, n);
+  }
+  return cuda_ok(ctx, cudaGetLastError(), "convert launch");
+}
+
+template <typename C>
+__global__ void k_split(const C* __restrict__ st, uint64_t off, uint64_t cnt, double* __restrict__ re,
+                        double* __restrict__ im) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    double2 v = tod<C>(st[off + i]);
+    re[i] = v.x;
+    im[i] = v.y;
+  }
+}
+
+}  // namespace cvdv
+
+// ====================================================================== C API
+static Context* C(CVDVContext* p) { return static_cast<Context*>(p); }
+
+static bool ready(Context* c, const char* what) {
+  if (c->numReg == 0 || !c->initialized) {
+    set_error(c, kErrNotInitialized, "%s: state not initialised", what);
+    return false;
+  }
+  return flush(c);
+}
+
+extern "C" {
+
+int cvdvGetLastError(CVDVContext* ctx, char* msg, int len);
+
+void cvdvGetState(CVDVContext* ctx, double* realOut, double* imagOut) {
+  if (!ctx) return;
+  Context* c = C(ctx);
+  if (!ready(c, "cvdvGetState") || !realOut || !imagOut) return;
+  uint64_t n = c->size();
+  const uint64_t chunk = 1ull << 22;
+  uint64_t cnt0 = n < chunk ? n : chunk;
+  double* dre = (double*)arena_alloc(c, cnt0 * sizeof(double));
+  double* dim = (double*)arena_alloc(c, cnt0 * sizeof(double));
+  if (!dre || !dim) return;
+  for (uint64_t off = 0; off < n; off += chunk) {
+    uint64_t cnt = n - off < chunk ? n - off : chunk;
+    int blocks = (int)((cnt + 255) / 256 < 1184 ? (cnt + 255) / 256 : 1184);
+    if (c->precision == kC128)
+      {
+        LaunchScope _ls(ctx, kKReduce);
+        k_split<double2><<<blocks, 256, 0, c->stream>>>((const double2*)c->state(), off, cnt, dre, dim);
+      }
+    else
+      {
+        LaunchScope _ls(ctx, kKReduce);
+        k_split<float2><<<blocks, 256, 0, c->stream>>>((const float2*)c->state(), off, cnt, dre, dim);
+      }
+    if (!cuda_ok(c, cudaMemcpyAsync(realOut + off, dre, cnt * sizeof(double), cudaMemcpyDeviceToHost,
+                                    c->stream), "getState copy re") ||
+        !cuda_ok(c, cudaMemcpyAsync(imagOut + off, dim, cnt * sizeof(double), cudaMemcpyDeviceToHost,
+                                    c->stream), "getState copy im"))
+      return;
+  }
+  cuda_ok(c, cudaStreamSynchronize(c->stream), "getState sync");
+}
+
+double cvdvGetNorm(CVDVContext* ctx) {
+  if (!ctx) return 0.0;
+  Context* c = C(ctx);
+  if (!ready(c, "cvdvGetNorm")) return 0.0;
+  arena_reset(c);
+  double2 r;
+  bool ok = c->precision == kC128
+                ? reduce(c, OpNorm<double2>{(const double2*)c->state()}, c->size(), &r)
+                : reduce(c, OpNorm<float2>{(const float2*)c->state()}, c->size(), &r);
+  return ok ? r.x : 0.0;
+}
+
+static bool measure(Context* c, const int* regIdxs, int numRegs, double* probsOut, const char* w) {
+  if (!regIdxs || numRegs <= 0 || !probsOut) {
+    set_error(c, kErrInvalidArg, "%s: empty register list", w);
+    return false;
+  }
+  if (numRegs > 16) {
+    set_error(c, kErrInvalidArg, "%s: at most 16 registers", w);
+    return false;
+  }
+  for (int s = 0; s < numRegs; ++s)
+    if (regIdxs[s] < 0 || regIdxs[s] >= c->numReg) {
+      set_error(c, kErrInvalidArg, "%s: invalid register index %d", w, regIdxs[s]);
+      return false;
+    }
+  if (!ready(c, w)) return false;
+  arena_reset(c);
+  double* dOut;
+  long long outSize;
+  if (!marginal_device(c, regIdxs, numRegs, &dOut, &outSize)) return false;
+  if (!cuda_ok(c, cudaMemcpyAsync(probsOut, dOut, (size_t)outSize * sizeof(double),
+                                  cudaMemcpyDeviceToHost, c->stream), "marginal copy"))
+    return false;
+  return cuda_ok(c, cudaStreamSynchronize(c->stream), "marginal sync");
+}
+
+void cvdvMeasureMultiple(CVDVContext* ctx, const int* regIdxs, int numRegs, double* probsOut) {
+  if (!ctx) return;
+  measure(C(ctx), regIdxs, numRegs, probsOut, "cvdvMeasureMultiple");
+}
+
+void cvdvMeasureMultipleCT(CVDVContext* ctx, const int* regIdxs, int numRegs, double* probsOut) {
+  if (!ctx) return;
+  measure(C(ctx), regIdxs, numRegs, probsOut, "cvdvMeasureMultipleCT");
+}
+
+void cvdvMeasureEach(CVDVContext* ctx, const int* regIdxs, int numRegs, double* probsOut) {
+  if (!ctx) return;
+  Context* c = C(ctx);
+  size_t off = 0;
+  for (int k = 0; k < numRegs; ++k) {
+    if (!measure(c, regIdxs + k, 1, probsOut + off, "cvdvMeasureEach")) return;
+    off += (size_t)1 << c->q[regIdxs[k]];
+  }
+}
+
+void cvdvGetFidelity(CVDVContext* ctx, void** devicePtrs, int numReg, double* fidOut) {
+  if (!ctx) return;
+  Context* c = C(ctx);
+  if (fidOut) *fidOut = 0.0;
+  if (!fidOut || !devicePtrs) {
+    set_error(c, kErrInvalidArg, "cvdvGetFidelity: NULL argument");
+    return;
+  }
+  if (numReg != c->numReg) {
+    set_error(c, kErrInvalidArg, "cvdvGetFidelity: numReg mismatch (context %d, got %d)",
+              c->numReg, numReg);
+    return;
+  }
+  if (!ready(c, "cvdvGetFidelity")) return;
+  arena_reset(c);
+  size_t totalN = 0;
+  for (int r = 0; r < numReg; ++r) totalN += (size_t)1 << c->q[r];
+  double2* base = (double2*)arena_alloc(c, totalN * sizeof(double2));
+  if (!base) return;
+  std::vector<const double2*> arrs(numReg);
+  size_t off = 0;
+  for (int r = 0; r < numReg; ++r) {
+    size_t N = (size_t)1 << c->q[r];
+    if (!cuda_ok(c, cudaMemcpyAsync(base + off, devicePtrs[r], N * sizeof(double2), cudaMemcpyDefault,
+                                    c->stream), "cvdvGetFidelity copy"))
+      return;
+    arrs[r] = base + off;
+    off += N;
+  }
+  // outer product of all registers but the last (same helper as the initialiser)
+  int R = c->numReg, qLast = c->q[R - 1];
+  uint64_t nOuter = 1ull << (c->totalQbt - qLast);
+  double2* outer = (double2*)arena_alloc(c, nOuter * sizeof(double2));
+  if (!outer) return;
+  if (!launch_outer(c, arrs.data(), outer)) return;
+  double2 ip;
+  bool ok = c->precision == kC128
+                ? reduce(c, OpSep<double2>{(const double2*)c->state(), outer, arrs[R - 1], qLast}, c->size(), &ip)
+                : reduce(c, OpSep<float2>{(const float2*)c->state(), outer, arrs[R - 1], qLast}, c->size(), &ip);
+  if (ok) *fidOut = ip.x * ip.x + ip.y * ip.y;
+}
+
+double cvdvGetPhotonNumber(CVDVContext* ctx, int regIdx) {
+  if (!ctx) return -1.0;
+  Context* c = C(ctx);
+  if (regIdx < 0 || regIdx >= c->numReg) {
+    set_error(c, kErrInvalidArg, "cvdvGetPhotonNumber: invalid register index %d", regIdx);
+    return -1.0;
+  }
+  if (!ready(c, "cvdvGetPhotonNumber")) return -1.0;
+  arena_reset(c);
+  int N = 1 << c->q[regIdx];
+  double cc = (double)(N - 1) * 0.5, dx = c->dx[regIdx];
+  int sh = c->flw[regIdx];
+  double2 q2, p2;
+  bool ok = c->precision == kC128
+                ? reduce(c, OpX2<double2>{(const double2*)c->state(), sh, N - 1, cc, dx}, c->size(), &q2)
+                : reduce(c, OpX2<float2>{(const float2*)c->state(), sh, N - 1, cc, dx}, c->size(), &q2);
+  if (!ok) return -1.0;
+  // <p^2>: |FtQ2P psi|^2 = |FFT(pre-twiddle * psi)|^2 / N, computed out of place
+  Term tw{};
+  tw.kind = kTermFtTw;
+  tw.r = regIdx;
+  tw.s = -1;
+  tw.ctrlBit = -1;
+  tw.sign = 1;
+  Term sc{};
+  sc.kind = kTermScalar;
+  sc.ctrlBit = -1;
+  sc.g0 = make_double2(1.0 / sqrt((double)N), 0.0);
+  FactorList pre;
+  std::vector<Term> left;
+  if (!build_factor_list(c, {tw, sc}, &pre, &left)) return -1.0;
+  size_t bytes = (size_t)c->size() * c->elemBytes;
+  char* scratch = (char*)big_scratch(c, bytes);
+  if (!scratch) return -1.0;
+  // the second state buffer is free between flushes: it serves as the pass temporary
+  if (!launch_fft_into(c, regIdx, 1, pre, scratch, c->other())) return -1.0;
+  ok = c->precision == kC128
+           ? reduce(c, OpX2<double2>{(const double2*)scratch, sh, N - 1, cc, dx}, c->size(), &p2)
+           : reduce(c, OpX2<float2>{(const float2*)scratch, sh, N - 1, cc, dx}, c->size(), &p2);
+  if (!ok) return -1.0;
+  return (q2.x + p2.x - 1.0) / 2.0;
+}
+
+void cvdvFidelityStatevectors(CVDVContext* ctx1, CVDVContext* ctx2, double* fidOut) {
+  if (fidOut) *fidOut = 0.0;
+  if (!ctx1 || !ctx2 || !fidOut) return;
+  Context* a = C(ctx1);
+  Context* b = C(ctx2);
+  if (a->totalQbt != b->totalQbt || a->numReg == 0 || b->numReg == 0) {
+    set_error(a, kErrInvalidArg, "cvdvFidelityStatevectors: total qubit count mismatch (%d vs %d)",
+              a->totalQbt, b->totalQbt);
+    return;
+  }
+  if (!ready(a, "cvdvFidelityStatevectors") || !ready(b, "cvdvFidelityStatevectors")) return;
+  if (a != b && !cuda_ok(b, cudaStreamSynchronize(b->stream), "fidelity sync")) return;
+  arena_reset(a);
+  double2 ip;
+  bool ok;
+  uint64_t n = a->size();
+  if (a->precision == kC128 && b->precision == kC128)
+    ok = reduce(a, OpDot<double2, double2>{(const double2*)a->state(), (const double2*)b->state()}, n, &ip);
+  else if (a->precision == kC128)
+    ok = reduce(a, OpDot<double2, float2>{(const double2*)a->state(), (const float2*)b->state()}, n, &ip);
+  else if (b->precision == kC128)
+    ok = reduce(a, OpDot<float2, double2>{(const float2*)a->state(), (const double2*)b->state()}, n, &ip);
+  else
+    ok = reduce(a, OpDot<float2, float2>{(const float2*)a->state(), (const float2*)b->state()}, n, &ip);
+  if (ok) *fidOut = ip.x * ip.x + ip.y * ip.y;
+}
+
+int cvdvGetLastError(CVDVContext* ctx, char* msg, int len) {
+  if (!ctx) return global_error(msg, len);
+  Context* c = C(ctx);
+  if (msg && len > 0) {
+    strncpy(msg, c->lastMsg.c_str(), (size_t)len - 1);
+    msg[len - 1] = 0;
+  }
+  return c->lastErr;
+}
+
+void cvdvClearError(CVDVContext* ctx) {
+  if (!ctx) return;
+  C(ctx)->lastErr = kOk;
+  C(ctx)->lastMsg.clear();
+}
+
+}  // extern "C"

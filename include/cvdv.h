@@ -1,0 +1,174 @@
+/*
+ * libcvdv (B200 build) -- C ABI of the dense CV-DV state-vector path.
+ *
+ * Drop-in for the reference CUDA-CVDV library: every function of the
+ * reference's src/cuda/api.h:14-61 is exported here with the same name,
+ * signature and argument meaning, so the reference's Python wrapper
+ * (src/cudaCvdv.py:29-74, which binds them with ctypes) loads this library
+ * unchanged.  Each declaration cites the reference entry point it replaces.
+ *
+ * Differences in error behaviour (the reference prints to stderr and returns,
+ * or throws a C++ exception through the C ABI on CUDA failures):
+ *   - no function here throws, traps or exits;
+ *   - invalid arguments leave the state untouched and record an error that
+ *     cvdvGetLastError() returns (the output buffers are not written, except
+ *     where the reference writes 0: cvdvGetFidelity / cvdvFidelityStatevectors);
+ *   - gates called before the state is initialised record an error instead of
+ *     running on an empty buffer.
+ *
+ * Execution: gates are queued on the context and run, fused, at the next
+ * readout (m / getState / Wigner / Husimi / fidelity / photon number / norm),
+ * at cvdvSetStateFromDevicePtr, or at cvdvSynchronize.  All device work of a
+ * context runs on one CUDA stream owned by the context; that stream is a
+ * blocking stream, so it is ordered with work on the legacy default stream.
+ * Readouts return after their results are on the host.  A context is not
+ * thread-safe (as in the reference).
+ */
+#ifndef CVDV_B200_H
+#define CVDV_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CVDVContext CVDVContext;
+
+/* ---------------------------------------------------------------- lifecycle */
+
+/* src/cuda/context.cu:7-67 (api.h:14).  Registers: numQubits[r] >= 1 each,
+ * sum <= 34.  complex128 state.  Returns NULL only if the host allocation
+ * fails; a context created with bad sizes has no registers and records an
+ * error. */
+CVDVContext* cvdvCreate(int numReg, int* numQubits);
+/* src/cuda/context.cu:70-72 (api.h:15). */
+void cvdvDestroy(CVDVContext* ctx);
+/* src/cuda/context.cu:117-129 (api.h:16): release device memory, keep the handle. */
+void cvdvFree(CVDVContext* ctx);
+/* src/cuda/context.cu:75-115 (api.h:17).  devicePtrs[r] points to N_r
+ * complex128 values (device or host memory); psi = tensor product, last
+ * register fastest, not normalised.  Built on the device. */
+void cvdvInitFromSeparable(CVDVContext* ctx, void** devicePtrs, int numReg);
+/* src/cuda/context.cu:131-137 (api.h:18).  d_src: 2^n complex128 values
+ * (device or host memory). */
+void cvdvSetStateFromDevicePtr(CVDVContext* ctx, void* d_src);
+/* src/cuda/context.cu:139-163 (api.h:19-23). */
+int cvdvGetNumRegisters(CVDVContext* ctx);
+size_t cvdvGetTotalSize(CVDVContext* ctx);
+void cvdvGetRegisterInfo(CVDVContext* ctx, int* qubitCountsOut, double* gridStepsOut);
+int cvdvGetRegisterDim(CVDVContext* ctx, int regIdx);
+double cvdvGetRegisterDx(CVDVContext* ctx, int regIdx);
+
+/* ---------------------------------------------------------------- gates */
+
+/* src/cuda/gates.cu:19-67 (api.h:25): centred DFT q -> p. */
+void cvdvFtQ2P(CVDVContext* ctx, int regIdx);
+/* src/cuda/gates.cu:69-122 (api.h:26): centred inverse DFT p -> q. */
+void cvdvFtP2Q(CVDVContext* ctx, int regIdx);
+/* src/cuda/gates.cu:124-161 (api.h:27). */
+void cvdvDisplacement(CVDVContext* ctx, int regIdx, double betaRe, double betaIm);
+/* src/cuda/gates.cu:163-204 (api.h:28-29). */
+void cvdvConditionalDisplacement(CVDVContext* ctx, int targetReg, int ctrlReg, int ctrlQubit,
+                                 double betaRe, double betaIm);
+/* src/cuda/gates.cu:206-219 (api.h:30); axis 0/1/2 = X/Y/Z. */
+void cvdvPauliRotation(CVDVContext* ctx, int regIdx, int qubitIdx, int axis, double theta);
+/* src/cuda/gates.cu:221-233 (api.h:31). */
+void cvdvHadamard(CVDVContext* ctx, int regIdx, int qubitIdx);
+/* src/cuda/gates.cu:235-246 (api.h:32). */
+void cvdvParity(CVDVContext* ctx, int regIdx);
+/* src/cuda/gates.cu:248-268 (api.h:33). */
+void cvdvConditionalParity(CVDVContext* ctx, int targetReg, int ctrlReg, int ctrlQubit);
+/* src/cuda/gates.cu:270-286 (api.h:34). */
+void cvdvSwapRegisters(CVDVContext* ctx, int reg1, int reg2);
+/* src/cuda/gates.cu:288-300 (api.h:35): exp(i t q^2). */
+void cvdvPhaseSquare(CVDVContext* ctx, int regIdx, double t);
+/* src/cuda/gates.cu:302-314 (api.h:36): exp(i t q^3). */
+void cvdvPhaseCubic(CVDVContext* ctx, int regIdx, double t);
+/* src/cuda/gates.cu:316-348 (api.h:37). */
+void cvdvRotation(CVDVContext* ctx, int regIdx, double theta);
+/* src/cuda/gates.cu:350-392 (api.h:38-39). */
+void cvdvConditionalRotation(CVDVContext* ctx, int targetReg, int ctrlReg, int ctrlQubit,
+                             double theta);
+/* src/cuda/gates.cu:394-421 (api.h:40). */
+void cvdvSqueeze(CVDVContext* ctx, int regIdx, double r);
+/* src/cuda/gates.cu:423-459 (api.h:41-42). */
+void cvdvConditionalSqueeze(CVDVContext* ctx, int targetReg, int ctrlReg, int ctrlQubit,
+                            double r);
+/* src/cuda/gates.cu:461-502 (api.h:43). */
+void cvdvBeamSplitter(CVDVContext* ctx, int reg1, int reg2, double theta);
+/* src/cuda/gates.cu:504-547 (api.h:44-45). */
+void cvdvConditionalBeamSplitter(CVDVContext* ctx, int reg1, int reg2, int ctrlReg, int ctrlQubit,
+                                 double theta);
+/* src/cuda/gates.cu:549-565 (api.h:46): exp(i coeff q1 q2). */
+void cvdvQ1Q2Gate(CVDVContext* ctx, int reg1, int reg2, double coeff);
+
+/* ---------------------------------------------------------------- readouts */
+
+/* src/cuda/bosonic.cu:103-132 (api.h:48): native N x N Wigner, row = p. */
+void cvdvGetWigner(CVDVContext* ctx, int regIdx, double* wignerOut);
+/* src/cuda/bosonic.cu:134-138 (api.h:49): Husimi Q (overlap route, falling
+ * back to the Wigner route under the same memory rule as the reference). */
+void cvdvGetHusimiQ(CVDVContext* ctx, int regIdx, double* husimiOut);
+/* src/cuda/bosonic.cu:140-144 (api.h:50). */
+void cvdvGetHusimiQOverlap(CVDVContext* ctx, int regIdx, double* husimiOut);
+/* src/cuda/bosonic.cu:146-150 (api.h:51). */
+void cvdvGetHusimiQWigner(CVDVContext* ctx, int regIdx, double* husimiOut);
+/* src/cuda/measure.cu:65-123 (api.h:53-54): joint marginal, first selected
+ * register fastest. */
+void cvdvMeasureMultiple(CVDVContext* ctx, const int* regIdxs, int numRegs, double* probsOut);
+/* src/cuda/measure.cu:125-256 (api.h:55-56): same result as
+ * cvdvMeasureMultiple (the reference computes it with cuTENSOR). */
+void cvdvMeasureMultipleCT(CVDVContext* ctx, const int* regIdxs, int numRegs, double* probsOut);
+/* src/cuda/measure.cu:258-274 (api.h:57). */
+void cvdvGetState(CVDVContext* ctx, double* realOut, double* imagOut);
+/* src/cuda/measure.cu:276-300 (api.h:58): sum |psi|^2 (not its square root). */
+double cvdvGetNorm(CVDVContext* ctx);
+/* src/cuda/measure.cu:302-318 (api.h:59): |<psi|prod_r phi_r>|^2. */
+void cvdvGetFidelity(CVDVContext* ctx, void** devicePtrs, int numReg, double* fidOut);
+/* src/cuda/measure.cu:320-331 (api.h:60): (<q^2> + <p^2> - 1) / 2.  The state
+ * is not modified (the reference transforms it to p and back). */
+double cvdvGetPhotonNumber(CVDVContext* ctx, int regIdx);
+/* src/cuda/measure.cu:333-366 (api.h:61): |<psi1|psi2>|^2. */
+void cvdvFidelityStatevectors(CVDVContext* ctx1, CVDVContext* ctx2, double* fidOut);
+
+/* ---------------------------------------------------------------- extensions
+ * No reference counterpart. */
+
+/* Precision of the state: 0 = complex128 (plain, the default of cvdvCreate),
+ * 1 = complex64 state with FP64 phase generation and FP64 reductions. */
+CVDVContext* cvdvCreateEx(int numReg, int* numQubits, int precision);
+int cvdvGetPrecision(CVDVContext* ctx);
+/* Last error of ctx (or of the process when ctx is NULL): returns the code
+ * (0 = none) and copies the message into msg[0..len). */
+int cvdvGetLastError(CVDVContext* ctx, char* msg, int len);
+void cvdvClearError(CVDVContext* ctx);
+/* Run every queued gate and wait for the context's stream. */
+void cvdvSynchronize(CVDVContext* ctx);
+/* Run every queued gate without waiting (enqueue only). */
+void cvdvFlush(CVDVContext* ctx);
+/* Number of gate stages currently queued. */
+int cvdvPendingStages(CVDVContext* ctx);
+/* Device pointer to the live state (complex128 or complex64 per precision),
+ * valid until the next gate flush; flushes first. */
+void* cvdvGetStateDevicePtr(CVDVContext* ctx);
+/* The context's CUDA stream (cudaStream_t). */
+void* cvdvGetStream(CVDVContext* ctx);
+/* Number of kernels this library has launched in the process so far. */
+unsigned long long cvdvLaunchCount(void);
+/* Per-launch timing: when on, every kernel launch of ctx is bracketed by a CUDA
+ * event pair.  cvdvGetKernelStats waits for the stream, returns the number of
+ * kernel kinds, fills total milliseconds and launch counts per kind
+ * (0 FFT pass, 1 qubit pair, 2 diagonal run, 3 permutation, 4 factor table,
+ * 5 initialiser, 6 reduction, 7 phase space) and resets them. */
+void cvdvSetTiming(CVDVContext* ctx, int on);
+int cvdvGetKernelStats(CVDVContext* ctx, double* msOut, long long* countOut, int n);
+/* Marginals of several single registers in one pass over the state:
+ * probsOut receives, for each k, dims[regIdxs[k]] values back to back. */
+void cvdvMeasureEach(CVDVContext* ctx, const int* regIdxs, int numRegs, double* probsOut);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CVDV_B200_H */

@@ -593,3 +593,109 @@ class OracleCvdv:
         F = F * np.exp(-0.25 * (wq * wq + wp * wp))
         out = np.fft.ifft2(F).real  # = unnormalised inverse / N^2
         return np.maximum(out, 0.0)
+
+
+class OracleSim(OracleCvdv):
+    """The oracle behind the ``CudaCvdv`` method names (``src/cudaCvdv.py:77-252``),
+    so one gate list drives both the CUDA library and the checker."""
+
+    def initStateVector(self, sep) -> None:
+        self.init_from_separable([np.asarray(a.cpu().numpy()) for a in sep.register_arrays])
+
+    def initFromArray(self, arr) -> None:
+        self.set_state(np.asarray(arr))
+
+    def getState(self):
+        return self.get_state()
+
+    def d(self, r, beta):
+        beta = complex(beta)
+        self.displacement(r, beta.real, beta.imag)
+
+    def cd(self, t, c, q, alpha):
+        alpha = complex(alpha)
+        self.cond_displacement(t, c, q, alpha.real, alpha.imag)
+
+    def cr(self, t, c, q, theta):
+        self.cond_rotation(t, c, q, theta)
+
+    def x(self, r, k):
+        self.pauli_rotation(r, k, 0, PI)
+
+    def y(self, r, k):
+        self.pauli_rotation(r, k, 1, PI)
+
+    def z(self, r, k):
+        self.pauli_rotation(r, k, 2, PI)
+
+    def rx(self, r, k, t):
+        self.pauli_rotation(r, k, 0, t)
+
+    def ry(self, r, k, t):
+        self.pauli_rotation(r, k, 1, t)
+
+    def rz(self, r, k, t):
+        self.pauli_rotation(r, k, 2, t)
+
+    def h(self, r, k):
+        self.hadamard(r, k)
+
+    def p(self, r):
+        self.parity(r)
+
+    def cp(self, t, c, q):
+        self.cparity(t, c, q)
+
+    def sheer(self, r, t):
+        self.phase_x2(r, t)
+
+    def phaseCubic(self, r, t):
+        self.phase_x3(r, t)
+
+    def r(self, r, theta):
+        self.rotation(r, theta)
+
+    def s(self, r, rr):
+        self.squeeze(r, rr)
+
+    def cs(self, t, c, q, rr):
+        self.cond_squeeze(t, c, q, rr)
+
+    def bs(self, a, b, theta):
+        self.beam_splitter(a, b, theta)
+
+    def cbs(self, a, b, c, q, theta):
+        self.cond_beam_splitter(a, b, c, q, theta)
+
+    def ftQ2P(self, r):
+        self.ft_q2p(r)
+
+    def ftP2Q(self, r):
+        self.ft_p2q(r)
+
+    def getWigner(self, r, bound=None):
+        W = self.wigner(r)
+        if bound is None:
+            return W
+        N, dx = self.dims[r], self.dx[r]
+        x = (np.arange(N) - (N - 1) / 2) * dx
+        p = (np.arange(N) - N / 2) * (PI / (N * dx))
+        return W[np.ix_(np.abs(p) <= bound, np.abs(x) <= bound)]
+
+    def getHusimiQ(self, r, bound=None):
+        Q = self.husimi(r)
+        if bound is None:
+            return Q
+        N, dx = self.dims[r], self.dx[r]
+        x = (np.arange(N) - (N - 1) / 2) * dx
+        p = (np.arange(N) - N / 2) * (2 * PI / (N * dx))
+        return Q[np.ix_(np.abs(p) <= bound, np.abs(x) <= bound)]
+
+    def getPhotonNumber(self, r):
+        return self.photon_number(r)
+
+    def getFidelity(self, sep):
+        return self.get_fidelity([np.asarray(a.cpu().numpy()) for a in sep.register_arrays])
+
+    def fidelityWith(self, other):
+        return self.fidelity_with(other)

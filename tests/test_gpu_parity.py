@@ -1,0 +1,328 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle and with the
+reference's own outputs (golden fixtures from TorchCvdv).
+
+Tolerances: the plain complex128 form must match to 1e-10 relative (state L2)
+and 1e-12 absolute on marginals / phase-space values; the complex64 form to
+2e-5 relative.
+"""
+
+import math
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from oracle.cvdv_oracle import OracleSim
+from tests.golden.cases import GATE_CASES
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+GATES = dict(np.load(os.path.join(GOLD, "gates.npz")))
+READ = dict(np.load(os.path.join(GOLD, "readouts.npz")))
+C1 = dict(np.load(os.path.join(GOLD, "c1.npz")))
+TORCH_DIVERGES = {"q1q2_rev"}  # see tests/test_oracle_golden.py
+PLAIN_TOL = 1e-10
+MIXED_TOL = 2e-5
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def make(qubits, psi, precision="complex128"):
+    from cvdv_b200 import CudaCvdv
+    sim = CudaCvdv(list(qubits), precision=precision, check_errors=True)
+    sim.initFromArray(psi)
+    return sim
+
+
+def oracle(qubits, psi):
+    o = OracleSim(list(qubits))
+    o.set_state(psi)
+    return o
+
+
+def run(sim, seq):
+    for meth, args in seq:
+        getattr(sim, meth)(*args)
+
+
+@pytest.mark.parametrize("name,qubits,seq", GATE_CASES, ids=[c[0] for c in GATE_CASES])
+def test_gate_plain(name, qubits, seq):
+    psi = GATES[f"{name}__in"]
+    sim = make(qubits, psi)
+    run(sim, seq)
+    out = sim.getState()
+    o = oracle(qubits, psi)
+    run(o, seq)
+    assert rel(out, o.get_state()) < PLAIN_TOL, name
+    if name not in TORCH_DIVERGES:
+        assert rel(out, GATES[f"{name}__out"]) < PLAIN_TOL, name
+
+
+@pytest.mark.parametrize("name,qubits,seq", GATE_CASES, ids=[c[0] for c in GATE_CASES])
+def test_gate_mixed(name, qubits, seq):
+    psi = GATES[f"{name}__in"]
+    sim = make(qubits, psi, "complex64")
+    run(sim, seq)
+    o = oracle(qubits, psi)
+    run(o, seq)
+    assert rel(sim.getState(), o.get_state()) < MIXED_TOL, name
+
+
+def test_c1_circuit():
+    from cvdv_b200 import CudaCvdv, SeparableState
+    sep = SeparableState([1, 10])  # cuda tensors, as the reference
+    sep.setZero(0)
+    sep.setCoherent(1, 2 + 1j)
+    np.testing.assert_allclose(sep.register_arrays[1].cpu().numpy(), C1["reg1"], atol=1e-15)
+    sim = CudaCvdv([1, 10], check_errors=True)
+    sim.initStateVector(sep)
+    for meth, args in [("h", (0, 0)), ("cd", (1, 0, 0, 1.5)), ("r", (1, 0.3)), ("s", (1, 0.2)), ("h", (0, 0))]:
+        getattr(sim, meth)(*args)
+    assert rel(sim.getState(), C1["state"]) < PLAIN_TOL
+    np.testing.assert_allclose(sim.m(0), C1["m0"], atol=1e-12)
+    np.testing.assert_allclose(sim.m(1), C1["m1"], atol=1e-12)
+    Wc = sim.getWigner(1, 5.0)
+    assert Wc.shape == (255, 128)
+    np.testing.assert_allclose(Wc, C1["wigner_b5"], atol=1e-12)
+    o = OracleSim([1, 10])
+    o.set_state(C1["state"])
+    np.testing.assert_allclose(sim.getHusimiQ(1), o.husimi(1), atol=1e-12)
+    np.testing.assert_allclose(sim.getHusimiQ(1, 5.0), C1["husimi_torch_b5"], atol=1e-6)
+    np.testing.assert_allclose(sim.getHusimiQWigner(1), o.husimi_wigner(1), atol=1e-12)
+
+
+def test_marginals():
+    q = [2, 3, 4]
+    sim = make(q, READ["m_state"])
+    for key, regs in (("m_0", (0,)), ("m_1", (1,)), ("m_2", (2,)), ("m_20", (2, 0)),
+                      ("m_012", (0, 1, 2)), ("m_10", (1, 0))):
+        np.testing.assert_allclose(sim.m(*regs), READ[key], atol=1e-14, err_msg=key)
+    assert abs(sim.m() - np.sum(np.abs(READ["m_state"]) ** 2)) < 1e-13
+    each = sim.mEach([0, 2])
+    np.testing.assert_allclose(each[0], READ["m_0"], atol=1e-14)
+    np.testing.assert_allclose(each[1], READ["m_2"], atol=1e-14)
+
+
+def test_large_marginal_global_path():
+    """> 4096 bins uses the global-atomic path."""
+    rng = np.random.default_rng(5)
+    q = [7, 6, 2]
+    psi = rng.standard_normal(1 << 15) + 1j * rng.standard_normal(1 << 15)
+    psi /= np.linalg.norm(psi)
+    sim = make(q, psi)
+    o = oracle(q, psi)
+    np.testing.assert_allclose(sim.m(0, 1), o.m(0, 1), atol=1e-14)
+    np.testing.assert_allclose(sim.m(2, 0, 1), o.m(2, 0, 1), atol=1e-14)
+
+
+def test_photon_number_and_state_untouched():
+    sim = make([7], READ["n_state"])
+    before = sim.getState()
+    assert abs(sim.getPhotonNumber(0) - float(READ["n_value"])) < 1e-12
+    np.testing.assert_array_equal(sim.getState(), before)
+
+
+def test_wigner_husimi_readouts():
+    sim = make([6, 1], READ["w_state"])
+    o = oracle([6, 1], READ["w_state"])
+    np.testing.assert_allclose(sim.getWigner(0), READ["w_wigner"], atol=1e-13)
+    np.testing.assert_allclose(sim.getHusimiQ(0), o.husimi(0), atol=1e-13)
+    sim3 = make([2, 5, 2], READ["w3_state"])
+    o3 = oracle([2, 5, 2], READ["w3_state"])
+    np.testing.assert_allclose(sim3.getWigner(1), READ["w3_wigner"], atol=1e-13)
+    np.testing.assert_allclose(sim3.getHusimiQ(1), o3.husimi(1), atol=1e-13)
+    np.testing.assert_allclose(sim3.getHusimiQWigner(1), o3.husimi_wigner(1), atol=1e-13)
+
+
+def test_fidelities():
+    from cvdv_b200 import SeparableState
+    q = [3, 6]
+    sep = SeparableState(q)
+    sep.setUniform(0)
+    sep.setCoherent(1, 0.7 - 0.3j)
+    rng = np.random.default_rng(11)
+    psi = rng.standard_normal(512) + 1j * rng.standard_normal(512)
+    psi /= np.linalg.norm(psi)
+    sim = make(q, psi)
+    o = oracle(q, psi)
+    assert abs(sim.getFidelity(sep) - o.getFidelity(sep)) < 1e-14
+    phi = rng.standard_normal(512) + 1j * rng.standard_normal(512)
+    phi /= np.linalg.norm(phi)
+    sim2 = make(q, phi)
+    o2 = oracle(q, phi)
+    assert abs(sim.fidelityWith(sim2) - o.fidelity_with(o2)) < 1e-14
+    # across precisions
+    sim3 = make(q, phi, "complex64")
+    assert abs(sim.fidelityWith(sim3) - o.fidelity_with(o2)) < 1e-6
+
+
+@pytest.mark.parametrize("qubits,reg", [([13, 3], 0), ([3, 13], 1), ([12, 2], 0), ([2, 12], 1),
+                                        ([14, 1], 0), ([1, 14], 1), ([5, 11, 2], 1), ([4, 4, 4, 4], 2)])
+def test_fft_layouts(qubits, reg):
+    """Single- and two-pass transforms on contiguous, inner and outer registers."""
+    rng = np.random.default_rng(sum(qubits) * 7 + reg)
+    n = sum(qubits)
+    psi = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    psi /= np.linalg.norm(psi)
+    for prec, tol in (("complex128", PLAIN_TOL), ("complex64", MIXED_TOL)):
+        sim = make(qubits, psi, prec)
+        o = oracle(qubits, psi)
+        sim.ftQ2P(reg)
+        o.ft_q2p(reg)
+        assert rel(sim.getState(), o.get_state()) < tol
+        sim.d(reg, 0.3 - 0.2j)
+        o.displacement(reg, 0.3, -0.2)
+        sim.ftP2Q(reg)
+        o.ft_p2q(reg)
+        assert rel(sim.getState(), o.get_state()) < tol
+
+
+@pytest.mark.parametrize("n_qubits,mode_qubits", [(3, 10), (4, 13), (2, 14)])
+def test_state_transfer_scaled(n_qubits, mode_qubits):
+    """The headline circuit at reduced size, plain and mixed."""
+    from cvdv_b200 import CudaCvdv
+    from cvdv_b200 import workloads as W
+    circ = W.state_transfer(n_qubits=n_qubits, mode_qubits=mode_qubits)
+    o = OracleSim(circ["qubits"])
+    o.initStateVector(W.separable_arrays(circ))
+    W.apply(o, circ["prep"] + circ["gates"])
+    ref = o.get_state()
+    for prec, tol in (("complex128", PLAIN_TOL), ("complex64", MIXED_TOL)):
+        sim = CudaCvdv(circ["qubits"], precision=prec, check_errors=True)
+        sim.initStateVector(W.separable_arrays(circ, device="cuda"))
+        W.apply(sim, circ["prep"] + circ["gates"])
+        assert rel(sim.getState(), ref) < tol, prec
+        for k in range(n_qubits):
+            np.testing.assert_allclose(sim.m(k), o.m(k), atol=10 * tol)
+
+
+def test_gaussian_network_scaled():
+    from cvdv_b200 import CudaCvdv
+    from cvdv_b200 import workloads as W
+    circ = W.gaussian_network(layers=6, mode_qubits=7)
+    o = OracleSim(circ["qubits"])
+    o.initStateVector(W.separable_arrays(circ))
+    W.apply(o, circ["prep"] + circ["gates"])
+    sim = CudaCvdv(circ["qubits"], check_errors=True)
+    sim.initStateVector(W.separable_arrays(circ, device="cuda"))
+    W.apply(sim, circ["prep"] + circ["gates"])
+    assert rel(sim.getState(), o.get_state()) < PLAIN_TOL
+    np.testing.assert_allclose(sim.getWigner(0), o.wigner(0), atol=1e-12)
+
+
+def test_identities_reference_core():
+    """Identities of the reference's tests/test_core.py at its sizes and tolerance."""
+    from cvdv_b200 import CudaCvdv, SeparableState
+    rng = np.random.default_rng(3)
+    for _ in range(3):
+        a = complex(rng.uniform(-2, 2), rng.uniform(-2, 2))
+        b = complex(rng.uniform(-2, 2), rng.uniform(-2, 2))
+        sim = CudaCvdv([10])
+        sep = SeparableState([10])
+        sep.setFock(0, 0)
+        sim.initStateVector(sep)
+        sim.d(0, b)
+        sim.d(0, a)
+        ref = SeparableState([10])
+        ref.setCoherent(0, a + b)
+        assert abs(sim.getFidelity(ref) - 1) < 1e-10
+    # FT eigenstates
+    for n in (0, 3, 11):
+        sim = CudaCvdv([10])
+        sep = SeparableState([10])
+        sep.setFock(0, n)
+        sim.initStateVector(sep)
+        sim.ftQ2P(0)
+        assert abs(sim.getFidelity(sep) - 1) < 1e-10
+        sim.ftP2Q(0)
+        assert abs(sim.getFidelity(sep) - 1) < 1e-10
+    # conditional displacement commutator
+    x, y = 0.41, -0.73
+    sim = CudaCvdv([1, 10])
+    sep = SeparableState([1, 10])
+    sep.setUniform(0)
+    sep.setFock(1, 0)
+    sim.initStateVector(sep)
+    sim.cd(1, 0, 0, x)
+    sim.d(1, 1j * y)
+    sim.cd(1, 0, 0, -x)
+    sim.d(1, -1j * y)
+    sim.rz(0, 0, 4 * x * y)
+    assert abs(sim.getFidelity(sep) - 1) < 1e-10
+    # beam splitter binomial populations
+    nF, th = 5, 1.3
+    sim = CudaCvdv([10, 10])
+    sep = SeparableState([10, 10])
+    sep.setFock(0, nF)
+    sep.setFock(1, 0)
+    sim.initStateVector(sep)
+    sim.bs(0, 1, th)
+    p1, p2 = math.cos(th / 2) ** 2, math.sin(th / 2) ** 2
+    for j in range(nF + 1):
+        s2 = SeparableState([10, 10])
+        s2.setFock(0, j)
+        s2.setFock(1, nF - j)
+        expect = math.comb(nF, j) * p1 ** j * p2 ** (nF - j)
+        assert abs(sim.getFidelity(s2) - expect) < 1e-10
+    # conditional rotation phase identity
+    nF, th = 7, 2.4
+    sim = CudaCvdv([1, 10])
+    sep = SeparableState([1, 10])
+    sep.setUniform(0)
+    sep.setFock(1, nF)
+    sim.initStateVector(sep)
+    sim.cr(1, 0, 0, th)
+    sim.rz(0, 0, th * -(2 * nF + 1))
+    assert abs(sim.getFidelity(sep) - 1) < 1e-10
+
+
+def test_errors_leave_state_untouched():
+    from cvdv_b200 import CudaCvdv
+    from cvdv_b200 import _lib
+    rng = np.random.default_rng(1)
+    psi = rng.standard_normal(64) + 0j
+    sim = CudaCvdv([3, 3])
+    sim.initFromArray(psi)
+    L = _lib.load()
+    L.cvdvDisplacement(sim.ctx, 5, 1.0, 0.0)
+    code, msg = sim.last_error()
+    assert code == 1 and "invalid register" in msg
+    L.cvdvClearError(sim.ctx)
+    L.cvdvSwapRegisters(sim.ctx, 0, 1)
+    L.cvdvHadamard(sim.ctx, 0, 3)  # qubit out of range
+    assert sim.last_error()[0] == 1
+    L.cvdvQ1Q2Gate(sim.ctx, 1, 1, 0.3)
+    assert sim.last_error()[0] == 1
+    np.testing.assert_allclose(sim.getState(), np.swapaxes(psi.reshape(8, 8), 0, 1).reshape(-1))
+    empty = CudaCvdv([2])
+    L.cvdvHadamard(empty.ctx, 0, 0)  # before init
+    assert empty.last_error()[0] == 2
+
+
+def test_full_size_state_transfer_properties():
+    """The 2^28-amplitude circuit: norm is conserved, qubit marginals sum to it,
+    and a forward/inverse transform pair of the mode returns the state."""
+    from cvdv_b200 import CudaCvdv
+    from cvdv_b200 import workloads as W
+    circ = W.state_transfer()
+    sim = CudaCvdv(circ["qubits"], check_errors=True)
+    sim.initStateVector(W.separable_arrays(circ, device="cuda"))
+    W.apply(sim, circ["prep"])
+    n0 = sim.m()
+    assert abs(n0 - 1.0) < 1e-6
+    W.apply(sim, circ["gates"])
+    n1 = sim.m()
+    assert abs(n1 - n0) < 1e-10
+    for k in range(14):
+        p = sim.m(k)
+        assert abs(p.sum() - n1) < 1e-10
+    before = sim.stateTensor().clone()
+    sim.ftQ2P(14)
+    sim.ftP2Q(14)
+    after = sim.stateTensor()
+    err = float(torch.linalg.vector_norm(after - before) / torch.linalg.vector_norm(before))
+    assert err < 1e-12
