@@ -200,13 +200,14 @@ def run_gpu(args, world, rank, local):
 
     torch.cuda.set_device(local)
     L = _lib.load()
-    circ = W.state_transfer()
+    # "small" (10 qubit registers, 2^24 amplitudes) exists for profiler captures
+    circ = W.state_transfer() if args.workload == "full" else W.state_transfer(n_qubits=10)
     G = len(circ["gates"])
     hbm, peak_kind = peaks()
     out = {}
 
-    def timed_run(precision):
-        sim = CudaCvdv(circ["qubits"], precision=precision, check_errors=True)
+    def timed_run(precision, fusion=True):
+        sim = CudaCvdv(circ["qubits"], precision=precision, check_errors=True, fusion=fusion)
         sim.initStateVector(W.separable_arrays(circ, device="cuda"))
         W.apply(sim, circ["prep"])
         sim.synchronize()
@@ -245,14 +246,27 @@ def run_gpu(args, world, rank, local):
 
     ms, stats, launches, clocks, norm = timed_run("complex128")
     n_amp = 1 << sum(circ["qubits"])
-    fft_ms, fft_n = stats["fft_pass"]
-    per_launch_ms = fft_ms / max(fft_n, 1)
-    # algorithmic bytes per FFT launch: the transform's one logical read+write of
-    # the state (2 * 2^n * 16 B), split over its passes (2 passes for 2^14)
-    passes = 2
-    alg_bytes = 2 * n_amp * 16 / passes
-    achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9
     total_kernel_ms = sum(v[0] for v in stats.values())
+    # Every kernel of this workload is one read + write of the state: the
+    # algorithmic bytes of a launch are 2 * 2^n * 16 B (complex128).
+    alg_bytes = 2 * n_amp * 16
+    KNAME = {"pair": "k_pair (H with the neighbouring diagonal runs: conditional phase in p, Rz)",
+             "fft_pass": "k_row (row program: mode DFT + diagonal runs, cluster of 4 CTAs)"}
+
+    def kern_roof(st, nbytes):
+        out = {}
+        for k in ("pair", "fft_pass"):
+            t, n = st[k]
+            if n:
+                per = t / n
+                out[k] = {"kernel": KNAME[k], "launches": n, "avg_launch_ms": per,
+                          "achieved_gbs": nbytes / (per * 1e-3) / 1e9,
+                          "share_of_kernel_time": t / max(sum(v[0] for v in st.values()), 1e-12)}
+        return out
+
+    kr = kern_roof(stats, alg_bytes)
+    dom = max(kr, key=lambda k: kr[k]["share_of_kernel_time"])
+    achieved = kr[dom]["achieved_gbs"]
     value = G * world / (ms * 1e-3)
 
     # ---- e2e through the public API with host buffers
@@ -279,11 +293,12 @@ def run_gpu(args, world, rank, local):
     del sim
     torch.cuda.empty_cache()
 
+    # ---- every transform executed (queue cancellation off), complex128
+    msnf, statsnf, launchesnf, _, normnf = timed_run("complex128", fusion=False)
+    krnf = kern_roof(statsnf, alg_bytes)
     # ---- mixed precision (complex64 state) on the same circuit
     ms64, stats64, launches64, clocks64, norm64 = timed_run("complex64")
-    f64_ms, f64_n = stats64["fft_pass"]
-    pl64 = f64_ms / max(f64_n, 1)
-    ach64 = (2 * n_amp * 8 / passes) / (pl64 * 1e-3) / 1e9
+    kr64 = kern_roof(stats64, alg_bytes // 2)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -294,19 +309,23 @@ def run_gpu(args, world, rank, local):
                    "l2": "state 4 GiB > L2 126 MB, no flush needed", "parallelism": f"replicas x{world}"},
         "amplitudes_per_s": value * n_amp,
         "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "kernel": "k_fft_pass (register FFT, 2 passes of radix 128)",
+        "roofline": {"bound": "hbm", "kernel": KNAME[dom],
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_kind": peak_kind, "traffic": None,
-                     "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": per_launch_ms,
-                     "launches": fft_n, "share_of_kernel_time": fft_ms / max(total_kernel_ms, 1e-12)},
+                     "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": kr[dom]["avg_launch_ms"],
+                     "launches": kr[dom]["launches"], "share_of_kernel_time": kr[dom]["share_of_kernel_time"],
+                     "kernels": kr},
         "kernel_ms_per_step": {k: v[0] / args.steps for k, v in stats.items() if v[1]},
         "clocks": clocks,
         "e2e": {"value": G * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "includes": "init from host arrays + 2 prep gates + 42 gates + 14 marginals"},
         "norm_after": norm,
+        "queue_fusion": "FtP2Q/FtQ2P pairs separated only by gates on other registers are cancelled "
+                        "(exact identity); see every_transform_executed for the run without it",
+        "every_transform_executed": {"value": G * world / (msnf * 1e-3), "ms_per_step": msnf,
+                                     "gpu_launches": int(launchesnf), "kernels": krnf, "norm_after": normnf},
         "mixed_c64": {"value": G * world / (ms64 * 1e-3), "ms_per_step": ms64, "gpu_launches": int(launches64),
-                      "roofline_frac": ach64 / hbm, "achieved_gbs": ach64, "norm_after": norm64,
-                      "speedup_vs_plain": ms / ms64},
+                      "kernels": kr64, "norm_after": norm64, "speedup_vs_plain": ms / ms64},
     }
     if world == 1 and rank == 0 and not args.no_cpu:
         threads = os.cpu_count() or 1
@@ -324,6 +343,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--workload", default="full", choices=["full", "small"],
+                    help="small: 10 qubit registers + the 2^14 mode (2^24 amplitudes), for ncu")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -86,25 +86,86 @@ double2 ft_global(int N, int sign, double scale) {
   return make_double2(scale * cos(a), scale * sin(a));
 }
 
+// Whether a queued stage leaves register r untouched (so it commutes with any
+// operator acting on r alone).
+bool touches_bit(Context* c, int r, int bit) {
+  return bit >= c->flw[r] && bit < c->flw[r] + c->q[r];
+}
+
+bool commutes_with_reg(Context* c, const Stage& s, int r) {
+  switch (s.kind) {
+    case kStDiag:
+      for (const Term& t : s.terms) {
+        if (t.kind == kTermScalar) continue;
+        if (t.r == r || (t.kind == kTermXX && t.s == r)) return false;
+        if (t.ctrlBit >= 0 && touches_bit(c, r, t.ctrlBit)) return false;
+      }
+      return true;
+    case kStFft:
+      return s.reg != r;
+    case kStPair:
+      return !touches_bit(c, r, s.bit);
+    case kStPerm:
+      if (s.reg == r || s.reg2 == r) return false;
+      return !(s.perm == kPermCondParity && touches_bit(c, r, s.bit));
+  }
+  return false;
+}
+
 void queue_ft(Context* c, int r, int dir) {
+  if (c->cancelFt) {
+    // FtQ2P(r) . FtP2Q(r) = FtP2Q(r) . FtQ2P(r) = I exactly (conjugate twiddles and
+    // global phases, unitary scale); stages in between that leave r alone commute.
+    for (int i = (int)c->pending.size() - 1; i >= 0; --i) {
+      const Stage& s = c->pending[i];
+      if (s.ftTag && s.ftReg == r) {
+        if (s.ftDir == -dir) {
+          int tag = s.ftTag;
+          std::vector<Stage> kept;
+          kept.reserve(c->pending.size());
+          for (Stage& t : c->pending)
+            if (t.ftTag != tag) kept.push_back(std::move(t));
+          c->pending.swap(kept);
+          ++c->ftCancelled;
+          return;
+        }
+        break;
+      }
+      if (!commutes_with_reg(c, s, r)) break;
+    }
+  }
   int N = 1 << c->q[r];
+  int tag = c->nextFtTag++;
   Term tw{};
   tw.kind = kTermFtTw;
   tw.r = r;
   tw.s = -1;
   tw.ctrlBit = -1;
   tw.sign = dir;
-  push_diag(c, {tw});
+  Stage pre;
+  pre.kind = kStDiag;
+  pre.terms = {tw};
   Stage f;
   f.kind = kStFft;
   f.reg = r;
   f.dir = dir;
-  push_stage(c, std::move(f));
   Term sc{};
   sc.kind = kTermScalar;
   sc.ctrlBit = -1;
   sc.g0 = ft_global(N, dir, 1.0 / sqrt((double)N));
-  push_diag(c, {tw, sc});
+  Stage post;
+  post.kind = kStDiag;
+  post.terms = {tw, sc};
+  for (Stage* s : {&pre, &f, &post}) {
+    s->ftTag = tag;
+    s->ftReg = r;
+    s->ftDir = dir;
+  }
+  // the three stages enter the queue together (a flush never splits them)
+  c->pending.push_back(std::move(pre));
+  c->pending.push_back(std::move(f));
+  c->pending.push_back(std::move(post));
+  if (c->pending.size() > 512) flush(c);
 }
 
 void queue_pair(Context* c, int bit, double2 m00, double2 m01, double2 m10, double2 m11) {
@@ -425,6 +486,13 @@ void* cvdvGetStateDevicePtr(CVDVContext* ctx) {
 void* cvdvGetStream(CVDVContext* ctx) { return ctx ? (void*)C(ctx)->stream : nullptr; }
 
 unsigned long long cvdvLaunchCount(void) { return cvdv::g_launches.load(); }
+
+void cvdvSetFusion(CVDVContext* ctx, int flags) {
+  if (!ctx) return;
+  C(ctx)->cancelFt = (flags & 1) != 0;
+}
+
+long long cvdvCancelledTransforms(CVDVContext* ctx) { return ctx ? C(ctx)->ftCancelled * 2 : 0; }
 
 void cvdvSetTiming(CVDVContext* ctx, int on) {
   if (!ctx) return;

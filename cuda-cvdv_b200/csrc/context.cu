@@ -317,9 +317,41 @@ static bool run_leftover(Context* ctx, std::vector<Term> terms) {
 }
 
 // ----------------------------------------------------------------- flush
+// Whether a diagonal run fits one factor list (no leftover).
+static bool diag_fits(Context* ctx, const std::vector<Term>& terms) {
+  std::vector<std::pair<int, int>> groups;
+  int nxx = 0;
+  std::vector<int> perGroup;
+  for (const Term& t : terms) {
+    if (t.kind == kTermScalar) continue;
+    if (t.kind == kTermXX) {
+      ++nxx;
+      continue;
+    }
+    int ctrl = -1;
+    if (t.kind == kTermPoly && t.ctrlBit >= 0) {
+      int lo = ctx->flw[t.r], hi = lo + ctx->q[t.r];
+      if (!(t.ctrlBit >= lo && t.ctrlBit < hi)) ctrl = t.ctrlBit;
+    }
+    std::pair<int, int> key{t.r, ctrl};
+    size_t g = 0;
+    while (g < groups.size() && groups[g] != key) ++g;
+    if (g == groups.size()) {
+      groups.push_back(key);
+      perGroup.push_back(0);
+    }
+    ++perGroup[g];
+  }
+  int tables = 0;
+  for (int c : perGroup) tables += (c + kMaxTermsPerTable - 1) / kMaxTermsPerTable;
+  return tables <= kMaxTab && nxx <= kMaxXX;
+}
+
 struct Op {
-  const Stage* st;
+  const Stage* st = nullptr;        // pass-kernel op (FFT pass / pair / permutation)
   std::vector<Term> pre, post;
+  int rowReg = -1;                  // row program on this register when >= 0
+  std::vector<HostRowOp> row;
 };
 
 bool flush(Context* ctx) {
@@ -334,17 +366,84 @@ bool flush(Context* ctx) {
   stages.swap(ctx->pending);
   std::vector<Op> ops;
   std::vector<Term> diag;
-  for (const Stage& s : stages) {
+  size_t i = 0;
+  while (i < stages.size()) {
+    const Stage& s = stages[i];
     if (s.kind == kStDiag) {
       diag.insert(diag.end(), s.terms.begin(), s.terms.end());
+      ++i;
       continue;
     }
-    ops.push_back({&s, diag, {}});
+    if (s.kind == kStFft && row_eligible(ctx, s.reg)) {
+      // a row program: every following FFT on this register and every diagonal
+      // run between / after them, in order, up to the program limits
+      Op op;
+      op.rowReg = s.reg;
+      int nDiag = 0;
+      auto addDiag = [&](const std::vector<Term>& t) -> bool {
+        if (!op.row.empty() && op.row.back().kind == kRowDiag) {
+          std::vector<Term> merged = op.row.back().terms;
+          merged.insert(merged.end(), t.begin(), t.end());
+          if (!row_diag_fits(ctx, s.reg, merged)) return false;
+          op.row.back().terms = std::move(merged);
+          return true;
+        }
+        if (nDiag >= kMaxRowDiags || (int)op.row.size() >= kMaxRowOps ||
+            !row_diag_fits(ctx, s.reg, t))
+          return false;
+        op.row.push_back({kRowDiag, 0, t});
+        ++nDiag;
+        return true;
+      };
+      if (!diag.empty() && !addDiag(diag)) {
+        run_leftover(ctx, diag);  // unusual: the leading run is too large; run it alone
+        op.row.clear();
+        nDiag = 0;
+      }
+      diag.clear();
+      size_t j = i;
+      while (j < stages.size()) {
+        const Stage& t = stages[j];
+        if (t.kind == kStFft && t.reg == s.reg) {
+          if ((int)op.row.size() + 2 > kMaxRowOps) break;
+          op.row.push_back({kRowFft, t.dir, {}});
+        } else if (t.kind == kStDiag) {
+          if (!addDiag(t.terms)) break;
+        } else {
+          break;
+        }
+        ++j;
+      }
+      ops.push_back(std::move(op));
+      i = j;
+      continue;
+    }
+    Op op;
+    op.st = &s;
+    op.pre = diag;
+    ops.push_back(std::move(op));
     diag.clear();
+    ++i;
   }
   if (ops.empty()) return run_leftover(ctx, diag);
-  ops.back().post = diag;
+  if (!diag.empty()) {
+    if (ops.back().rowReg >= 0) {
+      // (only reachable when the program hit its limits) run the tail alone
+      ops.push_back(Op{});
+      ops.back().pre = diag;
+    } else {
+      ops.back().post = diag;
+    }
+  }
   for (Op& op : ops) {
+    if (op.rowReg >= 0) {
+      if (!launch_row_program(ctx, op.rowReg, op.row)) return false;
+      continue;
+    }
+    if (!op.st) {  // standalone diagonal run
+      if (!run_leftover(ctx, op.pre)) return false;
+      continue;
+    }
     FactorList pre, post;
     std::vector<Term> lpre, lpost;
     if (!build_factor_list(ctx, op.pre, &pre, &lpre)) return false;

@@ -108,15 +108,24 @@ __device__ __forceinline__ double2 dmul(double2 a, double2 b) {
 
 // Evaluate the factor at flat index i (FP64).  Returns false when the list is
 // empty (factor == 1).
-__device__ __forceinline__ double2 eval_factor(const FactorList& F, uint64_t i) {
+template <int MAXT = kMaxTab, bool XX = true>
+__device__ __forceinline__ double2 eval_factor_t(const FactorList& F, uint64_t i) {
   double2 f = F.hasScalar ? F.scalar : make_double2(1.0, 0.0);
-#pragma unroll 1
-  for (int t = 0; t < F.nTab; ++t) {
-    const TabFactor& T = F.tab[t];
-    int j = (int)((i >> T.shift) & (uint64_t)T.mask);
-    if (T.ctrlShift >= 0) j += (int)((i >> T.ctrlShift) & 1ull) * T.half;
-    f = dmul(f, __ldg(T.ptr + j));
+  // issue every table load before the products so they overlap
+  double2 tv[MAXT];
+#pragma unroll
+  for (int t = 0; t < MAXT; ++t) {
+    if (t < F.nTab) {
+      const TabFactor& T = F.tab[t];
+      int j = (int)((i >> T.shift) & (uint64_t)T.mask);
+      if (T.ctrlShift >= 0) j += (int)((i >> T.ctrlShift) & 1ull) * T.half;
+      tv[t] = __ldg(T.ptr + j);
+    }
   }
+#pragma unroll
+  for (int t = 0; t < MAXT; ++t)
+    if (t < F.nTab) f = dmul(f, tv[t]);
+  if (!XX) return f;
 #pragma unroll 1
   for (int t = 0; t < F.nXX; ++t) {
     const XXFactor& X = F.xx[t];
@@ -131,6 +140,10 @@ __device__ __forceinline__ double2 eval_factor(const FactorList& F, uint64_t i) 
     f = dmul(f, make_double2(c, s));
   }
   return f;
+}
+
+__device__ __forceinline__ double2 eval_factor(const FactorList& F, uint64_t i) {
+  return eval_factor_t<kMaxTab, true>(F, i);
 }
 
 __host__ __device__ __forceinline__ bool factor_empty(const FactorList& F) {
@@ -162,6 +175,9 @@ enum PermKind : int { kPermParity = 0, kPermCondParity = 1, kPermSwap = 2 };
 
 struct Stage {
   int kind;
+  int ftTag = 0;      // > 0: one of the three stages of one FtQ2P / FtP2Q
+  int ftReg = -1;     // register of that basis change
+  int ftDir = 0;      // its direction (+1 FtQ2P, -1 FtP2Q)
   int reg = -1, reg2 = -1;
   int dir = 1;        // FFT: +1 forward (e^{-2 pi i jk/N}), -1 inverse (unnormalised)
   int bit = -1;       // pair: global bit; perm: control bit
@@ -237,6 +253,12 @@ struct Context {
   size_t hostScratchCap = 0;
 
   std::vector<Stage> pending;
+  // Basis-change cancellation: FtQ2P(r) after FtP2Q(r) (or the reverse) with only
+  // stages that leave register r untouched in between is the identity; both are
+  // dropped from the queue.  On by default (cvdvSetFusion).
+  bool cancelFt = true;
+  int nextFtTag = 1;
+  long long ftCancelled = 0;
 
   int lastErr = kOk;
   std::string lastMsg;
@@ -275,6 +297,10 @@ bool build_factor_list(Context* ctx, const std::vector<Term>& terms, FactorList*
 // kernel launchers (kernels_*.cu); all enqueue on ctx->stream
 bool launch_build_table(Context* ctx, int r, bool ctrl, const Term* terms, int nTerms,
                         double2* out);
+// permLogC > 0 stores the table permuted for a cluster of 2^permLogC CTAs in the
+// transposed layout: position rank * (N >> permLogC) + m holds index rank + (m << permLogC)
+bool launch_build_table_ext(Context* ctx, int r, int nExt, const int* extBits, const Term* terms,
+                            int nTerms, double2* out, int permLogC = 0);
 bool launch_diag(Context* ctx, const FactorList& F);
 bool launch_pair(Context* ctx, int bit, const double2 m[4], const FactorList& pre,
                  const FactorList& post);
@@ -283,6 +309,19 @@ bool launch_fft(Context* ctx, int reg, int dir, const FactorList& pre, const Fac
 bool launch_fft_generic(Context* ctx, const void* in, void* out, void* tmp, uint64_t O,
                         int q, uint64_t S, int dir, int prec);
 bool launch_init_product(Context* ctx, const double2* const* regArrays);
+
+// row programs (kernels_row.cu): FFTs and diagonal runs on the contiguous register
+constexpr int kMaxRowOps = 24;
+constexpr int kMaxRowDiags = 10;
+enum RowOpKind : int { kRowDiag = 0, kRowFft = 1 };
+struct HostRowOp {
+  int kind;
+  int dir;
+  std::vector<Term> terms;
+};
+bool row_eligible(Context* ctx, int reg);
+bool row_diag_fits(Context* ctx, int reg, const std::vector<Term>& terms);
+bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops);
 // outer[h] = prod over registers but the last of phi_r[j_r(h)], h < 2^(n - q_last)
 bool launch_outer(Context* ctx, const double2* const* regArrays, double2* outer);
 // FFT of the live state along `reg` into `out` (state untouched); `tmp` is the

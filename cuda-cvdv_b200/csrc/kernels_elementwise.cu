@@ -23,7 +23,9 @@ struct TTerm {
 
 struct TableJob {
   int N;
-  int ctrl;        // 1: table has two halves indexed by an external control bit
+  int ctrl;        // number of external control bits: the table has 2^ctrl segments
+  int permLogC;    // > 0: entries stored permuted (see launch_build_table_ext)
+  int permLogM;
   double dx;
   int nTerms;
   TTerm t[kMaxTermsPerTable];
@@ -36,10 +38,11 @@ struct TableJob {
 // twiddle is generated exactly from the integer (N-1)(2j-N+1) mod 4N so its
 // argument carries no rounding however large N is.
 __global__ void k_build_table(TableJob job, double2* out) {
-  int total = job.N * (job.ctrl ? 2 : 1);
+  int total = job.N << job.ctrl;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
     int j = e % job.N;
     int b = e / job.N;
+    if (job.permLogC) j = ((j & ((1 << job.permLogM) - 1)) << job.permLogC) + (j >> job.permLogM);
     double x = ((double)j - (double)(job.N - 1) * 0.5) * job.dx;
     double ph = 0.0;
     bool anyPoly = false;
@@ -51,7 +54,8 @@ __global__ void k_build_table(TableJob job, double2* out) {
         if (T.power == 1) v = T.coeff * x;
         else if (T.power == 2) v = T.coeff * x * x;
         else v = T.coeff * x * x * x;
-        bool neg = (T.ctrlMode == 1 && b == 1) || (T.ctrlMode == 2 && ((j >> T.ctrlLocal) & 1));
+        bool neg = (T.ctrlMode == 1 && ((b >> T.ctrlLocal) & 1)) ||
+                   (T.ctrlMode == 2 && ((j >> T.ctrlLocal) & 1));
         ph += neg ? -v : v;
         anyPoly = true;
       } else if (T.kind == kTermFtTw) {
@@ -76,11 +80,15 @@ __global__ void k_build_table(TableJob job, double2* out) {
   }
 }
 
-bool launch_build_table(Context* ctx, int r, bool ctrl, const Term* terms, int nTerms,
-                        double2* out) {
+// Table over register r with nExt external control bits (extBits, flat-index
+// positions outside r): entry [seg][j], seg bit c = value of extBits[c].
+bool launch_build_table_ext(Context* ctx, int r, int nExt, const int* extBits, const Term* terms,
+                            int nTerms, double2* out, int permLogC) {
   TableJob job{};
   job.N = 1 << ctx->q[r];
-  job.ctrl = ctrl ? 1 : 0;
+  job.ctrl = nExt;
+  job.permLogC = permLogC;
+  job.permLogM = ctx->q[r] - permLogC;
   job.dx = ctx->dx[r];
   job.nTerms = nTerms;
   int lo = ctx->flw[r], hi = ctx->flw[r] + ctx->q[r];
@@ -102,10 +110,12 @@ bool launch_build_table(Context* ctx, int r, bool ctrl, const Term* terms, int n
         D.ctrlLocal = T.ctrlBit - lo;
       } else {
         D.ctrlMode = 1;
+        for (int c = 0; c < nExt; ++c)
+          if (extBits[c] == T.ctrlBit) D.ctrlLocal = c;
       }
     }
   }
-  int total = job.N * (ctrl ? 2 : 1);
+  int total = job.N << nExt;
   int threads = 256;
   int blocks = (total + threads - 1) / threads;
   if (blocks > 1184) blocks = 1184;
@@ -114,6 +124,19 @@ bool launch_build_table(Context* ctx, int r, bool ctrl, const Term* terms, int n
     k_build_table<<<blocks, threads, 0, ctx->stream>>>(job, out);
   }
   return cuda_ok(ctx, cudaGetLastError(), "build_table launch");
+}
+
+bool launch_build_table(Context* ctx, int r, bool ctrl, const Term* terms, int nTerms,
+                        double2* out) {
+  int bit = -1;
+  if (ctrl) {
+    int lo = ctx->flw[r], hi = lo + ctx->q[r];
+    for (int t = 0; t < nTerms; ++t)
+      if (terms[t].kind == kTermPoly && terms[t].ctrlBit >= 0 &&
+          !(terms[t].ctrlBit >= lo && terms[t].ctrlBit < hi))
+        bit = terms[t].ctrlBit;
+  }
+  return launch_build_table_ext(ctx, r, ctrl ? 1 : 0, &bit, terms, nTerms, out);
 }
 
 // ----------------------------------------------------------------- diag run
@@ -163,49 +186,86 @@ bool launch_diag(Context* ctx, const FactorList& F) {
 
 // ----------------------------------------------------------------- pair (2x2)
 // Pair indexing as qubitPairIndices (src/cuda/kernels/utils.cuh:79-84).
-template <typename C>
+// Each thread takes kPairV pairs per iteration, all loads issued first.  The
+// factor-free instance (the common case: neighbouring diagonal runs usually
+// ride on a row program) is a separate, lean specialisation.
+constexpr int kPairV = 4;
+
+// MAXT: 0 = no factors; 2 = at most two tables and no bilinear terms (the
+// usual neighbouring run: a qubit phase and one mode table); kMaxTab = general.
+template <typename C, int MAXT>
 __global__ void __launch_bounds__(256) k_pair(C* __restrict__ st, uint64_t npairs, int bit,
                                              double2 m00, double2 m01, double2 m10, double2 m11,
-                                             FactorList pre, FactorList post) {
-  const bool hasPre = !factor_empty(pre), hasPost = !factor_empty(post);
+                                             const __grid_constant__ FactorList pre,
+                                             const __grid_constant__ FactorList post) {
+  constexpr int V = MAXT == 0 ? kPairV : (MAXT == 2 ? 2 : 1);
+  constexpr bool XX = MAXT == kMaxTab;
   const uint64_t lowMask = (1ull << bit) - 1;
   const C a00 = fromd<C>(m00), a01 = fromd<C>(m01), a10 = fromd<C>(m10), a11 = fromd<C>(m11);
-  for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < npairs;
-       p += (uint64_t)gridDim.x * blockDim.x) {
-    uint64_t i0 = ((p & ~lowMask) << 1) | (p & lowMask);
-    uint64_t i1 = i0 | (1ull << bit);
-    C a = st[i0], b = st[i1];
-    if (hasPre) {
-      a = cmul(a, fromd<C>(eval_factor(pre, i0)));
-      b = cmul(b, fromd<C>(eval_factor(pre, i1)));
+  const bool hasPre = MAXT > 0 && !factor_empty(pre), hasPost = MAXT > 0 && !factor_empty(post);
+  const uint64_t step = (uint64_t)gridDim.x * blockDim.x * V;
+  for (uint64_t p0 = (uint64_t)blockIdx.x * blockDim.x * V + threadIdx.x; p0 < npairs;
+       p0 += step) {
+    C a[V], b[V];
+    uint64_t i0[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      uint64_t p = p0 + (uint64_t)v * blockDim.x;
+      i0[v] = ((p & ~lowMask) << 1) | (p & lowMask);
+      if (p < npairs) {
+        a[v] = st[i0[v]];
+        b[v] = st[i0[v] | (1ull << bit)];
+      }
     }
-    C na = cadd(cmul(a00, a), cmul(a01, b));
-    C nb = cadd(cmul(a10, a), cmul(a11, b));
-    if (hasPost) {
-      na = cmul(na, fromd<C>(eval_factor(post, i0)));
-      nb = cmul(nb, fromd<C>(eval_factor(post, i1)));
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      uint64_t p = p0 + (uint64_t)v * blockDim.x;
+      if (p >= npairs) continue;
+      uint64_t i1 = i0[v] | (1ull << bit);
+      C x = a[v], y = b[v];
+      if constexpr (MAXT > 0) {
+        if (hasPre) {
+          x = cmul(x, fromd<C>(eval_factor_t<(MAXT > 0 ? MAXT : 1), XX>(pre, i0[v])));
+          y = cmul(y, fromd<C>(eval_factor_t<(MAXT > 0 ? MAXT : 1), XX>(pre, i1)));
+        }
+      }
+      C nx = cadd(cmul(a00, x), cmul(a01, y));
+      C ny = cadd(cmul(a10, x), cmul(a11, y));
+      if constexpr (MAXT > 0) {
+        if (hasPost) {
+          nx = cmul(nx, fromd<C>(eval_factor_t<(MAXT > 0 ? MAXT : 1), XX>(post, i0[v])));
+          ny = cmul(ny, fromd<C>(eval_factor_t<(MAXT > 0 ? MAXT : 1), XX>(post, i1)));
+        }
+      }
+      st[i0[v]] = nx;
+      st[i1] = ny;
     }
-    st[i0] = na;
-    st[i1] = nb;
   }
+}
+
+template <typename C>
+static void pair_launch(Context* ctx, uint64_t np, int bit, const double2 m[4],
+                        const FactorList& pre, const FactorList& post) {
+  LaunchScope _ls(ctx, kKPair);
+  bool none = factor_empty(pre) && factor_empty(post);
+  bool small = pre.nTab <= 2 && post.nTab <= 2 && pre.nXX == 0 && post.nXX == 0;
+  C* st = (C*)ctx->state();
+  if (none)
+    k_pair<C, 0><<<grid_for(np, 256, kPairV), 256, 0, ctx->stream>>>(st, np, bit, m[0], m[1], m[2],
+                                                                      m[3], pre, post);
+  else if (small)
+    k_pair<C, 2><<<grid_for(np, 256, 2), 256, 0, ctx->stream>>>(st, np, bit, m[0], m[1], m[2],
+                                                                m[3], pre, post);
+  else
+    k_pair<C, kMaxTab><<<grid_for(np, 256, 1), 256, 0, ctx->stream>>>(st, np, bit, m[0], m[1],
+                                                                      m[2], m[3], pre, post);
 }
 
 bool launch_pair(Context* ctx, int bit, const double2 m[4], const FactorList& pre,
                  const FactorList& post) {
   uint64_t np = ctx->size() / 2;
-  int blocks = grid_for(np, 256, 2);
-  if (ctx->precision == kC128)
-    {
-      LaunchScope _ls(ctx, kKPair);
-      k_pair<double2><<<blocks, 256, 0, ctx->stream>>>((double2*)ctx->state(), np, bit, m[0], m[1],
-                                                       m[2], m[3], pre, post);
-    }
-  else
-    {
-      LaunchScope _ls(ctx, kKPair);
-      k_pair<float2><<<blocks, 256, 0, ctx->stream>>>((float2*)ctx->state(), np, bit, m[0], m[1],
-                                                      m[2], m[3], pre, post);
-    }
+  if (ctx->precision == kC128) pair_launch<double2>(ctx, np, bit, m, pre, post);
+  else pair_launch<float2>(ctx, np, bit, m, pre, post);
   return cuda_ok(ctx, cudaGetLastError(), "pair launch");
 }
 

@@ -151,24 +151,46 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_pass(const C* __restrict__ 
   const bool doPost = P.last && !factor_empty(post);
   const int total = R << P.logB;
 
-  // ---- load (memory order: inner b, t, outer b)
+  // ---- load (memory order: inner b, t, outer b).  All of a thread's loads are
+  // issued before any is used, so each thread keeps kFftPerThread requests in
+  // flight.
   {
     const int Wl = 1 << P.logWl;
-    for (int l = threadIdx.x; l < total; l += kFftThreads) {
-      int inner = l & (Wl - 1);
-      int t = (l >> P.logWl) & (R - 1);
-      int b = ((l >> (P.logWl + P.logR)) << P.logWl) | inner;
-      uint64_t c = c0 + b;
-      uint64_t s = c & Smask;
-      uint64_t tmp = c >> P.logS;
-      uint64_t jj = tmp & NRmask;
-      uint64_t o = tmp >> logNR;
-      uint64_t addr = (((o << P.logN) + jj + ((uint64_t)t << logNR)) << P.logS) + s;
-      C v = in[addr];
-      if (doPre) v = cmul(v, fromd<C>(eval_factor(pre, addr)));
-      int jm = (int)(jj & nsMask);
-      if (jm && t) v = cmul(v, twiddle<C, DIR>(P.tw, (jm * t) << P.twShift));
-      sm[b * RP + padt(t)] = v;
+    C v[kFftPerThread];
+#pragma unroll
+    for (int k = 0; k < kFftPerThread; ++k) {
+      int l = threadIdx.x + k * kFftThreads;
+      if (l < total) {
+        int inner = l & (Wl - 1);
+        int t = (l >> P.logWl) & (R - 1);
+        int b = ((l >> (P.logWl + P.logR)) << P.logWl) | inner;
+        uint64_t c = c0 + b;
+        uint64_t tmp = c >> P.logS;
+        uint64_t addr = ((((tmp >> logNR) << P.logN) + (tmp & NRmask) + ((uint64_t)t << logNR))
+                         << P.logS) + (c & Smask);
+        v[k] = in[addr];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kFftPerThread; ++k) {
+      int l = threadIdx.x + k * kFftThreads;
+      if (l < total) {
+        int inner = l & (Wl - 1);
+        int t = (l >> P.logWl) & (R - 1);
+        int b = ((l >> (P.logWl + P.logR)) << P.logWl) | inner;
+        uint64_t c = c0 + b;
+        uint64_t tmp = c >> P.logS;
+        uint64_t jj = tmp & NRmask;
+        C x = v[k];
+        if (doPre) {
+          uint64_t addr = ((((tmp >> logNR) << P.logN) + jj + ((uint64_t)t << logNR)) << P.logS) +
+                          (c & Smask);
+          x = cmul(x, fromd<C>(eval_factor(pre, addr)));
+        }
+        int jm = (int)(jj & nsMask);
+        if (jm && t) x = cmul(x, twiddle<C, DIR>(P.tw, (jm * t) << P.twShift));
+        sm[b * RP + padt(t)] = x;
+      }
     }
   }
   __syncthreads();
@@ -189,21 +211,25 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_pass(const C* __restrict__ 
   // ---- store (autosorted position)
   {
     const int Ws = 1 << P.logWs;
-    for (int l = threadIdx.x; l < total; l += kFftThreads) {
-      int inner = l & (Ws - 1);
-      int t = (l >> P.logWs) & (R - 1);
-      int b = ((l >> (P.logWs + P.logR)) << P.logWs) | inner;
-      uint64_t c = c0 + b;
-      uint64_t s = c & Smask;
-      uint64_t tmp = c >> P.logS;
-      uint64_t jj = tmp & NRmask;
-      uint64_t o = tmp >> logNR;
-      uint64_t k = ((jj >> P.logNs) << (P.logNs + P.logR)) + (jj & (uint64_t)nsMask) +
-                   ((uint64_t)t << P.logNs);
-      uint64_t addr = (((o << P.logN) + k) << P.logS) + s;
-      C v = sm[b * RP + padt(t)];
-      if (doPost) v = cmul(v, fromd<C>(eval_factor(post, addr)));
-      out[addr] = v;
+#pragma unroll
+    for (int kk = 0; kk < kFftPerThread; ++kk) {
+      int l = threadIdx.x + kk * kFftThreads;
+      if (l < total) {
+        int inner = l & (Ws - 1);
+        int t = (l >> P.logWs) & (R - 1);
+        int b = ((l >> (P.logWs + P.logR)) << P.logWs) | inner;
+        uint64_t c = c0 + b;
+        uint64_t s = c & Smask;
+        uint64_t tmp = c >> P.logS;
+        uint64_t jj = tmp & NRmask;
+        uint64_t o = tmp >> logNR;
+        uint64_t k = ((jj >> P.logNs) << (P.logNs + P.logR)) + (jj & (uint64_t)nsMask) +
+                     ((uint64_t)t << P.logNs);
+        uint64_t addr = (((o << P.logN) + k) << P.logS) + s;
+        C v = sm[b * RP + padt(t)];
+        if (doPost) v = cmul(v, fromd<C>(eval_factor(post, addr)));
+        out[addr] = v;
+      }
     }
   }
 }

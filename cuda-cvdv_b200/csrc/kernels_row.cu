@@ -1,0 +1,740 @@
+// Row programs: a run of basis changes and diagonal gates on the contiguous
+// (last) register, executed in ONE read + write of the state.
+//
+// A conditional displacement is FtQ2P . CPhaseX . FtP2Q (src/cuda/gates.cu:163-204);
+// the reference spends 9 elementwise passes and two cuFFT transforms on it.
+// Here the whole sequence -- pre-twiddle, forward DFT, post-twiddle / scale /
+// phase kick / next pre-twiddle, inverse DFT, post-twiddle / scale and any
+// following diagonal gates -- runs on a row held on chip.
+//
+// Tiling.  A CTA holds a tile of 4096 (complex128, 256 threads) or 8192
+// (complex64, 512 threads) amplitudes, 16 per thread, in one of two
+// shared-memory buffers (stages read one and write the other).  A register of
+// N <= tile points is processed as tile/N whole rows per CTA.  A longer row is
+// split across a thread-block cluster of C = N / tile CTAs (C = 2 or 4): CTA c
+// holds the contiguous chunk [c M, (c+1) M), M = N / C, and the DFT of the row
+// is one radix-C butterfly across the cluster (operands read from the other
+// CTAs' shared memory, DSMEM) plus an M-point DFT inside each CTA:
+//   forward  X[k1 + C k2] = sum_m w_M^{m k2} [ w_N^{m k1} sum_j1 w_C^{j1 k1} x[j1 M + m] ]
+//            -> CTA k1 holds X[k1 + C k2] at local position k2 ("transposed");
+//   inverse  x[j1 M + m]  = sum_k1 w_C^{-j1 k1} w_N^{-m k1} sum_k2 w_M^{-m k2} X[k1 + C k2]
+//            -> consumes the transposed layout and returns the natural one,
+// so FFT . diag . IFFT never reshuffles data between CTAs; a program that ends
+// in the transposed layout is redistributed once before the store.
+//
+// The M-point DFT runs as Stockham stages of radix 16 (plus one radix-2/4/8
+// stage when log2 M is not a multiple of 4).  Twiddles come from two small
+// shared-memory tables (w^e = hi[e >> 6] lo[e & 63]) and, inside a butterfly,
+// from powers of its base twiddle.  A diagonal run is applied as
+//   (per-row scalar) x (combined table of the row register)[ctrl segment][k]
+// where the per-row scalar collects every factor that does not depend on the
+// row register (qubit phases, other modes) and is computed once per row.
+
+#include <cooperative_groups.h>
+
+#include "cvdv_internal.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace cvdv {
+
+constexpr int kRowMinLogN = 8;  // shorter registers use the pass kernels
+
+template <typename C> struct RowCfg;
+template <> struct RowCfg<double2> {
+  static constexpr int LOGT = 8;  // 256 threads x 16 amplitudes (tile 4096)
+  static constexpr int LOGE = 4;
+  static constexpr int E = 16;
+};
+template <> struct RowCfg<float2> {
+  static constexpr int LOGT = 8;  // 256 threads x 32 amplitudes (tile 8192)
+  static constexpr int LOGE = 5;
+  static constexpr int E = 32;
+};
+
+struct RowOp {
+  int kind;
+  int dir;   // fft: +1 forward, -1 inverse
+  int diag;  // diag: index into RowProgram::diag
+};
+
+struct RowDiag {
+  const double2* tab;  // [2^nCtrl][N] combined factor of the row register, or null
+  int permuted;        // tab stored as [seg][rank][m] for k = rank + C m (transposed layout)
+  int nCtrl;
+  int ctrlShift[2];    // flat-index bits selecting the table segment (row bits)
+  int hasRowF, hasElemF;
+  FactorList rowF;     // factors constant along a row
+  FactorList elemF;    // per-element factors (bilinear terms with the row register)
+};
+
+struct RowProgram {
+  int logN;     // register length
+  int logM;     // row elements held by one CTA
+  int logRows;  // rows per CTA (cluster size 1 only)
+  int nOps;
+  int nDiag;
+  int logTwN;
+  const double2* tw;
+  RowOp ops[kMaxRowOps];
+  RowDiag diag[kMaxRowDiags];
+};
+
+// shared-memory position of element e of a row: one padding slot every 16
+// (the radix-16 stride), which keeps the strided butterfly accesses conflict-free
+template <typename C>
+__device__ __forceinline__ int rpad(int e) {
+  return e + (e >> 4);
+}
+
+// ---------------------------------------------------------------- butterflies
+template <typename C, int DIR>
+__device__ __forceinline__ C rot_mi(C a) {  // * (-DIR i)
+  return DIR > 0 ? mk(a.y, -a.x) : mk(-a.y, a.x);
+}
+
+template <typename C, int DIR>
+__device__ __forceinline__ void bf2(C& a, C& b) {
+  C t = a;
+  a = cadd(t, b);
+  b = csub(t, b);
+}
+
+template <typename C, int DIR>
+__device__ __forceinline__ void bf4(C& a0, C& a1, C& a2, C& a3) {
+  C s02 = cadd(a0, a2), d02 = csub(a0, a2);
+  C s13 = cadd(a1, a3), d13 = rot_mi<C, DIR>(csub(a1, a3));
+  a0 = cadd(s02, s13);
+  a2 = csub(s02, s13);
+  a1 = cadd(d02, d13);
+  a3 = csub(d02, d13);
+}
+
+// multiply by w8^K, w8 = exp(-DIR i pi / 4)
+template <typename C, int DIR, int K>
+__device__ __forceinline__ C w8mul(C o) {
+  using T = decltype(o.x);
+  const T h = (T)0.70710678118654752440;
+  if constexpr (K == 0) return o;
+  else if constexpr (K == 1)
+    return DIR > 0 ? mk(h * (o.x + o.y), h * (o.y - o.x)) : mk(h * (o.x - o.y), h * (o.y + o.x));
+  else if constexpr (K == 2) return rot_mi<C, DIR>(o);
+  else
+    return DIR > 0 ? mk(h * (o.y - o.x), -h * (o.x + o.y)) : mk(-h * (o.x + o.y), h * (o.x - o.y));
+}
+
+template <typename C, int DIR>
+__device__ __forceinline__ void bf8(C* v) {
+  C e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+  C o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+  bf4<C, DIR>(e0, e1, e2, e3);
+  bf4<C, DIR>(o0, o1, o2, o3);
+  o1 = w8mul<C, DIR, 1>(o1);
+  o2 = w8mul<C, DIR, 2>(o2);
+  o3 = w8mul<C, DIR, 3>(o3);
+  v[0] = cadd(e0, o0);
+  v[4] = csub(e0, o0);
+  v[1] = cadd(e1, o1);
+  v[5] = csub(e1, o1);
+  v[2] = cadd(e2, o2);
+  v[6] = csub(e2, o2);
+  v[3] = cadd(e3, o3);
+  v[7] = csub(e3, o3);
+}
+
+// radix 16 = 4 x 4: y[k1 + 4 k2] = sum_n2 w4^{n2 k2} [ w16^{n2 k1} sum_n1 w4^{n1 k1} x[4 n1 + n2] ]
+template <typename C, int DIR>
+__device__ __forceinline__ void bf16(C* v) {
+  using T = decltype(v[0].x);
+  const T c1 = (T)0.92387953251128675613, s1 = (T)0.38268343236508977173;
+  const T sg = DIR > 0 ? (T)-1 : (T)1;  // sign of the imaginary part of w16
+  C a[16];
+#pragma unroll
+  for (int n2 = 0; n2 < 4; ++n2) {
+    C x0 = v[n2], x1 = v[4 + n2], x2 = v[8 + n2], x3 = v[12 + n2];
+    bf4<C, DIR>(x0, x1, x2, x3);
+    a[n2 * 4 + 0] = x0;
+    a[n2 * 4 + 1] = x1;
+    a[n2 * 4 + 2] = x2;
+    a[n2 * 4 + 3] = x3;
+  }
+  auto mulw = [&](C x, T c, T s) { return mk(x.x * c - x.y * s, x.x * s + x.y * c); };
+  a[5] = mulw(a[5], c1, sg * s1);     // w^1
+  a[6] = w8mul<C, DIR, 1>(a[6]);      // w^2
+  a[7] = mulw(a[7], s1, sg * c1);     // w^3
+  a[9] = w8mul<C, DIR, 1>(a[9]);      // w^2
+  a[10] = rot_mi<C, DIR>(a[10]);      // w^4
+  a[11] = w8mul<C, DIR, 3>(a[11]);    // w^6
+  a[13] = mulw(a[13], s1, sg * c1);   // w^3
+  a[14] = w8mul<C, DIR, 3>(a[14]);    // w^6
+  a[15] = mulw(a[15], -c1, -sg * s1); // w^9 = -w^1
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1) {
+    C y0 = a[k1], y1 = a[4 + k1], y2 = a[8 + k1], y3 = a[12 + k1];
+    bf4<C, DIR>(y0, y1, y2, y3);
+    v[k1 + 0] = y0;
+    v[k1 + 4] = y1;
+    v[k1 + 8] = y2;
+    v[k1 + 12] = y3;
+  }
+}
+
+template <typename C, int DIR, int RHO>
+__device__ __forceinline__ void bfly(C* v) {
+  if constexpr (RHO == 16) bf16<C, DIR>(v);
+  else if constexpr (RHO == 8) bf8<C, DIR>(v);
+  else if constexpr (RHO == 4) bf4<C, DIR>(v[0], v[1], v[2], v[3]);
+  else bf2<C, DIR>(v[0], v[1]);
+}
+
+// ---------------------------------------------------------------- twiddles in smem
+// w_L^e = hi[e >> 6] * lo[e & 63] for e < L (L = M for the CTA-local DFT, N for
+// the cross-cluster butterfly); forward convention exp(-2 pi i e / L).
+struct TwTables {
+  double2* loM;
+  double2* hiM;
+  double2* loN;
+  double2* hiN;
+};
+
+template <typename C, int DIR>
+__device__ __forceinline__ C tw2(const double2* lo, const double2* hi, int e) {
+  double2 a = hi[e >> 6], b = lo[e & 63];
+  double2 w = make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+  if (DIR < 0) w.y = -w.y;
+  return fromd<C>(w);
+}
+
+// One Stockham stage of radix RHO, in place on the single tile buffer: every
+// thread gathers its butterflies' operands into registers, the CTA syncs, and
+// the results are scattered to their autosorted positions.
+template <typename C, int DIR, int RHO>
+__device__ __forceinline__ void row_stage(C* sm, int RS, int logM, int logNs, const TwTables& T) {
+  constexpr int LOGRHO = RHO == 16 ? 4 : (RHO == 8 ? 3 : (RHO == 4 ? 2 : 1));
+  constexpr int NT = 1 << RowCfg<C>::LOGT;
+  constexpr int K = RowCfg<C>::E / RHO;  // butterflies per thread
+  const int logNbf = logM - LOGRHO;
+  const int ns = 1 << logNs;
+  const int sc = logM - (logNs + LOGRHO);  // w_{ns RHO}^x = w_M^{x << sc}
+  C v[K][RHO];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    int bf = threadIdx.x + k * NT;
+    int row = bf >> logNbf;
+    int jb = bf & ((1 << logNbf) - 1);
+    const C* col = sm + row * RS;
+#pragma unroll
+    for (int u = 0; u < RHO; ++u) v[k][u] = col[rpad<C>(jb + (u << logNbf))];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    int bf = threadIdx.x + k * NT;
+    int row = bf >> logNbf;
+    int jb = bf & ((1 << logNbf) - 1);
+    int jm = jb & (ns - 1);
+    if (jm) {
+      C w1 = tw2<C, DIR>(T.loM, T.hiM, jm << sc);
+      C w = w1;
+      v[k][1] = cmul(v[k][1], w);
+#pragma unroll
+      for (int u = 2; u < RHO; ++u) {
+        w = cmul(w, w1);
+        v[k][u] = cmul(v[k][u], w);
+      }
+    }
+    bfly<C, DIR, RHO>(v[k]);
+    C* out = sm + row * RS;
+    int base = ((jb >> logNs) << (logNs + LOGRHO)) + jm;
+#pragma unroll
+    for (int u = 0; u < RHO; ++u) out[rpad<C>(base + u * ns)] = v[k][u];
+  }
+  __syncthreads();
+}
+
+// M-point DFT of every row segment of the tile
+template <typename C, int DIR>
+__device__ void local_fft(C* sm, int RS, int logM, const TwTables& T) {
+  int logNs = 0, rem = logM;
+  while (rem >= 4) {
+    row_stage<C, DIR, 16>(sm, RS, logM, logNs, T);
+    logNs += 4;
+    rem -= 4;
+  }
+  if (rem == 3) row_stage<C, DIR, 8>(sm, RS, logM, logNs, T);
+  else if (rem == 2) row_stage<C, DIR, 4>(sm, RS, logM, logNs, T);
+  else if (rem == 1) row_stage<C, DIR, 2>(sm, RS, logM, logNs, T);
+}
+
+// ---------------------------------------------------------------- cross-CTA steps
+// Each step reads the cluster peers' tiles (DSMEM) into registers, waits until
+// every CTA has read, then overwrites its own tile.
+// forward DIF radix-C butterfly: this CTA produces output k1 = rank at every m
+template <typename C, int LOGC>
+__device__ void cross_forward(C* sm, const TwTables& T) {
+  constexpr int NC = 1 << LOGC;
+  constexpr int NT = 1 << RowCfg<C>::LOGT;
+  constexpr int E = RowCfg<C>::E;
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  cl.sync();  // every chunk of the row is complete
+  const C* peer[NC];
+#pragma unroll
+  for (int j = 0; j < NC; ++j) peer[j] = cl.map_shared_rank(sm, j);
+  C y[E];
+#pragma unroll
+  for (int k = 0; k < E; ++k) {
+    int m = threadIdx.x + k * NT;
+    int p = rpad<C>(m);
+    C x[NC];
+#pragma unroll
+    for (int j = 0; j < NC; ++j) x[j] = peer[j][p];
+    C acc;  // sum_j1 w_C^{j1 rank} x_j1
+    if constexpr (NC == 2) {
+      acc = rank ? csub(x[0], x[1]) : cadd(x[0], x[1]);
+    } else {
+      C s02 = cadd(x[0], x[2]), d02 = csub(x[0], x[2]);
+      C s13 = cadd(x[1], x[3]), d13 = rot_mi<C, 1>(csub(x[1], x[3]));
+      acc = rank == 0 ? cadd(s02, s13) : rank == 1 ? cadd(d02, d13) : rank == 2 ? csub(s02, s13) : csub(d02, d13);
+    }
+    int e = m * rank;  // w_N^{m rank}
+    y[k] = e ? cmul(acc, tw2<C, 1>(T.loN, T.hiN, e)) : acc;
+    if ((k & 7) == 7) asm volatile("" ::: "memory");  // bound the loads in flight
+  }
+  cl.sync();  // all reads of every tile are done
+#pragma unroll
+  for (int k = 0; k < E; ++k) sm[rpad<C>(threadIdx.x + k * NT)] = y[k];
+  __syncthreads();
+}
+
+// inverse DIT radix-C butterfly: this CTA (rank = j1) produces x[j1 M + m]
+template <typename C, int LOGC>
+__device__ void cross_inverse(C* sm, const TwTables& T) {
+  constexpr int NC = 1 << LOGC;
+  constexpr int NT = 1 << RowCfg<C>::LOGT;
+  constexpr int E = RowCfg<C>::E;
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  cl.sync();
+  const C* peer[NC];
+#pragma unroll
+  for (int j = 0; j < NC; ++j) peer[j] = cl.map_shared_rank(sm, j);
+  C y[E];
+#pragma unroll
+  for (int k = 0; k < E; ++k) {
+    int m = threadIdx.x + k * NT;
+    int p = rpad<C>(m);
+    C z[NC];
+    z[0] = peer[0][p];
+    C w1 = m ? tw2<C, -1>(T.loN, T.hiN, m) : fromd<C>(make_double2(1.0, 0.0));
+    C w = w1;  // z_k1 * w_N^{-m k1}
+#pragma unroll
+    for (int k1 = 1; k1 < NC; ++k1) {
+      z[k1] = cmul(peer[k1][p], w);
+      if (k1 + 1 < NC) w = cmul(w, w1);
+    }
+    C acc;  // sum_k1 w_C^{-rank k1} z_k1
+    if constexpr (NC == 2) {
+      acc = rank ? csub(z[0], z[1]) : cadd(z[0], z[1]);
+    } else {
+      C s02 = cadd(z[0], z[2]), d02 = csub(z[0], z[2]);
+      C s13 = cadd(z[1], z[3]), d13 = rot_mi<C, -1>(csub(z[1], z[3]));
+      acc = rank == 0 ? cadd(s02, s13) : rank == 1 ? cadd(d02, d13) : rank == 2 ? csub(s02, s13) : csub(d02, d13);
+    }
+    y[k] = acc;
+    if ((k & 7) == 7) asm volatile("" ::: "memory");  // bound the loads in flight
+  }
+  cl.sync();
+#pragma unroll
+  for (int k = 0; k < E; ++k) sm[rpad<C>(threadIdx.x + k * NT)] = y[k];
+  __syncthreads();
+}
+
+// layout change: natural (CTA j1 holds k = j1 M + m) <-> transposed (CTA k1 holds k = k1 + C m)
+template <typename C, int LOGC>
+__device__ void redistribute(C* sm, int logM, bool toNatural) {
+  constexpr int NC = 1 << LOGC;
+  constexpr int NT = 1 << RowCfg<C>::LOGT;
+  constexpr int E = RowCfg<C>::E;
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  cl.sync();
+  C y[E];
+#pragma unroll
+  for (int k = 0; k < E; ++k) {
+    int m = threadIdx.x + k * NT;
+    int kk, srcRank, srcPos;
+    if (toNatural) {
+      kk = (rank << logM) + m;
+      srcRank = kk & (NC - 1);
+      srcPos = kk >> LOGC;
+    } else {
+      kk = rank + (m << LOGC);
+      srcRank = kk >> logM;
+      srcPos = kk & ((1 << logM) - 1);
+    }
+    y[k] = cl.map_shared_rank(sm, srcRank)[rpad<C>(srcPos)];
+    if ((k & 7) == 7) asm volatile("" ::: "memory");  // bound the loads in flight
+  }
+  cl.sync();
+#pragma unroll
+  for (int k = 0; k < E; ++k) sm[rpad<C>(threadIdx.x + k * NT)] = y[k];
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------- the kernel
+// Single-CTA rows run two CTAs per SM (one loads while the other computes);
+// cluster rows hold the cross-step operands in registers and get the full file.
+template <typename C, int LOGC>
+__global__ void __launch_bounds__(1 << RowCfg<C>::LOGT, LOGC > 0 ? 1 : 2)
+    k_row(const C* __restrict__ in, C* __restrict__ out, const __grid_constant__ RowProgram P) {
+  constexpr int LOGT = RowCfg<C>::LOGT;
+  constexpr int NT = 1 << LOGT;
+  constexpr int E = RowCfg<C>::E;
+  constexpr int TILE = NT * E;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int logM = P.logM;
+  const int M = 1 << logM;
+  const int RS = rpad<C>(M);
+  const int rows = 1 << P.logRows;
+  C* sm = reinterpret_cast<C*>(smraw);
+  double2* twbase = reinterpret_cast<double2*>(sm + RS * rows);
+  TwTables T;
+  T.loM = twbase;
+  T.hiM = T.loM + 64;
+  T.loN = T.hiM + 128;
+  T.hiN = T.loN + 64;
+  double2* rowScalar = T.hiN + 512;  // [rows][nDiag]
+  int* rowSeg = reinterpret_cast<int*>(rowScalar + rows * P.nDiag);
+
+  int rank = 0;
+  uint64_t base;  // flat index of element 0 of this CTA's first row
+  if (LOGC == 0) {
+    base = (uint64_t)blockIdx.x * TILE;
+  } else {
+    rank = (int)cg::this_cluster().block_rank();
+    base = ((uint64_t)blockIdx.x >> LOGC) << P.logN;
+  }
+  const uint64_t chunk = base + ((uint64_t)rank << logM);  // first element held here
+
+  const bool headDiag = P.nOps > 0 && P.ops[0].kind == kRowDiag;
+  const bool tailDiag = P.nOps > 1 && P.ops[P.nOps - 1].kind == kRowDiag;
+  const int opEnd = tailDiag ? P.nOps - 1 : P.nOps;
+
+  // ---- twiddle tables and per-row diagonal scalars
+  {
+    const int scM = P.logTwN - logM, scN = P.logTwN - P.logN;
+    for (int i = threadIdx.x; i < 64 + 128 + 64 + 512; i += NT) {
+      double2 w = make_double2(1.0, 0.0);
+      if (i < 64) { if (i < M) w = __ldg(P.tw + ((size_t)i << scM)); }
+      else if (i < 192) { int h = i - 64; if ((h << 6) < M) w = __ldg(P.tw + ((size_t)(h << 6) << scM)); }
+      else if (i < 256) { int l = i - 192; if (LOGC && l < (1 << P.logN)) w = __ldg(P.tw + ((size_t)l << scN)); }
+      else { int h = i - 256; if (LOGC && (h << 6) < (1 << P.logN)) w = __ldg(P.tw + ((size_t)(h << 6) << scN)); }
+      twbase[i] = w;
+    }
+    for (int i = threadIdx.x; i < rows * P.nDiag; i += NT) {
+      int r = i / P.nDiag, d = i - r * P.nDiag;
+      const RowDiag& D = P.diag[d];
+      uint64_t rb = base + ((uint64_t)r << P.logN);
+      rowScalar[i] = D.hasRowF ? eval_factor(D.rowF, rb) : make_double2(1.0, 0.0);
+      int seg = 0;
+      for (int c = 0; c < D.nCtrl; ++c) seg |= (int)((rb >> D.ctrlShift[c]) & 1ull) << c;
+      rowSeg[i] = seg << P.logN;
+    }
+  }
+  __syncthreads();
+
+  bool transposed = false;
+  // table entry of diag d for tile element (row, m): the table of an op that
+  // runs in the transposed layout is stored permuted, so every read is contiguous
+  auto tab_at = [&](int d, int row, int m) -> double2 {
+    const RowDiag& D = P.diag[d];
+    if (!D.tab) return make_double2(1.0, 0.0);
+    int k = LOGC == 0 ? m : (rank << logM) + m;
+    return __ldg(D.tab + rowSeg[row * P.nDiag + d] + k);
+  };
+  auto factor_with = [&](int d, int row, int m, double2 t) -> C {
+    const RowDiag& D = P.diag[d];
+    double2 f = dmul(rowScalar[row * P.nDiag + d], t);
+    if (D.hasElemF) {
+      int k = LOGC == 0 ? m : (transposed ? rank + (m << LOGC) : (rank << logM) + m);
+      f = dmul(f, eval_factor(D.elemF, base + ((uint64_t)row << P.logN) + (uint64_t)k));
+    }
+    return fromd<C>(f);
+  };
+
+  // ---- load the tile: all E requests in flight per thread
+  {
+    C v[E];
+#pragma unroll
+    for (int k = 0; k < E; ++k) v[k] = in[chunk + threadIdx.x + k * NT];
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+      int e = threadIdx.x + k * NT;
+      sm[(e >> logM) * RS + rpad<C>(e & (M - 1))] = v[k];
+    }
+  }
+  __syncthreads();
+
+  for (int o = 0; o < opEnd; ++o) {
+    const RowOp op = P.ops[o];
+    if (op.kind == kRowDiag) {
+#pragma unroll 1
+      for (int k0 = 0; k0 < E; k0 += 8) {
+        double2 t[8];  // 8 table reads in flight before any is used
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          int e = threadIdx.x + (k0 + k) * NT;
+          t[k] = tab_at(op.diag, e >> logM, e & (M - 1));
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          int e = threadIdx.x + (k0 + k) * NT;
+          int row = e >> logM, m = e & (M - 1);
+          C* p = sm + row * RS + rpad<C>(m);
+          *p = cmul(*p, factor_with(op.diag, row, m, t[k]));
+        }
+      }
+      __syncthreads();
+    } else if (op.dir > 0) {
+      if constexpr (LOGC > 0) {
+        if (transposed) redistribute<C, LOGC>(sm, logM, true);
+        cross_forward<C, LOGC>(sm, T);
+        transposed = true;
+      }
+      local_fft<C, 1>(sm, RS, logM, T);
+    } else {
+      if constexpr (LOGC > 0) {
+        if (!transposed) {
+          redistribute<C, LOGC>(sm, logM, false);
+          transposed = true;
+        }
+      }
+      local_fft<C, -1>(sm, RS, logM, T);
+      if constexpr (LOGC > 0) {
+        cross_inverse<C, LOGC>(sm, T);
+        transposed = false;
+      }
+    }
+  }
+  if constexpr (LOGC > 0) {
+    if (transposed) {
+      redistribute<C, LOGC>(sm, logM, true);
+      transposed = false;
+    }
+  }
+
+  // ---- store (trailing diagonal run applied on the way out)
+  if (tailDiag) {
+    const int dd = P.ops[P.nOps - 1].diag;
+#pragma unroll 1
+    for (int k0 = 0; k0 < E; k0 += 8) {
+      double2 t[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        int e = threadIdx.x + (k0 + k) * NT;
+        t[k] = tab_at(dd, e >> logM, e & (M - 1));
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        int e = threadIdx.x + (k0 + k) * NT;
+        int row = e >> logM, m = e & (M - 1);
+        out[chunk + e] = cmul(sm[row * RS + rpad<C>(m)], factor_with(dd, row, m, t[k]));
+      }
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+      int e = threadIdx.x + k * NT;
+      out[chunk + e] = sm[(e >> logM) * RS + rpad<C>(e & (M - 1))];
+    }
+  }
+  if constexpr (LOGC > 0) cg::this_cluster().sync();  // no CTA leaves while peers may read it
+}
+
+// ---------------------------------------------------------------- host side
+int row_log_tile(int precision) { return precision == kC128 ? 12 : 13; }
+
+bool row_eligible(Context* ctx, int reg) {
+  if (ctx->flw[reg] != 0) return false;
+  int lt = row_log_tile(ctx->precision);
+  int q = ctx->q[reg];
+  if (q > lt + 2 || q < kRowMinLogN) return false;
+  if (ctx->totalQbt < lt) return false;  // tile larger than the state
+  return true;
+}
+
+// Split a diagonal run for a row program on `reg`.  Returns false when it does
+// not fit (more than two control bits on the row register, too many terms, or a
+// remainder that does not fit one factor list).
+static bool split_row_diag(Context* ctx, int reg, const std::vector<Term>& terms,
+                           std::vector<Term>* regTerms, std::vector<int>* ctrlBits,
+                           std::vector<Term>* rowTerms, std::vector<Term>* elemTerms) {
+  int lo = ctx->flw[reg], hi = lo + ctx->q[reg];
+  auto inReg = [&](int bit) { return bit >= lo && bit < hi; };
+  for (const Term& t : terms) {
+    if (t.kind == kTermXX) {
+      // bilinear terms touching the row register (or controlled from it) vary along the row
+      if (t.r == reg || t.s == reg || (t.ctrlBit >= 0 && inReg(t.ctrlBit))) elemTerms->push_back(t);
+      else rowTerms->push_back(t);
+      continue;
+    }
+    if (t.kind != kTermScalar && t.r == reg) {
+      if (t.kind == kTermPoly && t.ctrlBit >= 0 && !inReg(t.ctrlBit)) {
+        bool found = false;
+        for (int c : *ctrlBits) found |= c == t.ctrlBit;
+        if (!found) ctrlBits->push_back(t.ctrlBit);
+      }
+      regTerms->push_back(t);
+      continue;
+    }
+    if (t.kind == kTermPoly && t.ctrlBit >= 0 && inReg(t.ctrlBit)) {
+      elemTerms->push_back(t);  // another register's phase controlled by a row qubit
+      continue;
+    }
+    rowTerms->push_back(t);
+  }
+  if (ctrlBits->size() > 2 || regTerms->size() > (size_t)kMaxTermsPerTable) return false;
+  // rowTerms and elemTerms must each fit one factor list
+  auto fits = [&](const std::vector<Term>& ts) {
+    std::vector<std::pair<int, int>> groups;
+    std::vector<int> counts;
+    int nxx = 0;
+    for (const Term& t : ts) {
+      if (t.kind == kTermScalar) continue;
+      if (t.kind == kTermXX) {
+        ++nxx;
+        continue;
+      }
+      int c = -1;
+      if (t.kind == kTermPoly && t.ctrlBit >= 0) {
+        int l2 = ctx->flw[t.r], h2 = l2 + ctx->q[t.r];
+        if (!(t.ctrlBit >= l2 && t.ctrlBit < h2)) c = t.ctrlBit;
+      }
+      std::pair<int, int> key{t.r, c};
+      size_t g = 0;
+      while (g < groups.size() && groups[g] != key) ++g;
+      if (g == groups.size()) {
+        groups.push_back(key);
+        counts.push_back(0);
+      }
+      ++counts[g];
+    }
+    int tables = 0;
+    for (int n : counts) tables += (n + kMaxTermsPerTable - 1) / kMaxTermsPerTable;
+    return tables <= kMaxTab && nxx <= kMaxXX;
+  };
+  return fits(*rowTerms) && fits(*elemTerms);
+}
+
+bool row_diag_fits(Context* ctx, int reg, const std::vector<Term>& terms) {
+  std::vector<Term> a, b, c;
+  std::vector<int> bits;
+  return split_row_diag(ctx, reg, terms, &a, &bits, &b, &c);
+}
+
+template <typename C, int LOGC>
+static cudaError_t launch_row_t(Context* ctx, const RowProgram& P, uint64_t nCta, size_t smem) {
+  auto kern = k_row<C, LOGC>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)nCta);
+  cfg.blockDim = dim3(1u << RowCfg<C>::LOGT);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 1u << LOGC;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, (const C*)ctx->state(), (C*)ctx->other(), P);
+}
+
+bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops) {
+  RowProgram P{};
+  int lt = row_log_tile(ctx->precision);
+  int q = ctx->q[reg];
+  int logC = q > lt ? q - lt : 0;
+  P.logN = q;
+  P.logM = q - logC;
+  P.logRows = q < lt ? lt - q : 0;
+  P.logTwN = 0;
+  while ((1 << P.logTwN) < ctx->twN) ++P.logTwN;
+  P.tw = ctx->twiddle;
+  // layout at every op: a forward FFT leaves the cluster transposed, an inverse
+  // natural; the head diag runs at load and the tail diag after the final
+  // redistribution, both natural
+  bool transposedSim = false;
+  int opIndex = -1;
+  for (const HostRowOp& h : ops) {
+    ++opIndex;
+    bool isHead = opIndex == 0, isTail = opIndex + 1 == (int)ops.size() && opIndex > 0;
+    bool opTransposed = logC > 0 && transposedSim && !isHead && !isTail;
+    if (h.kind == kRowFft) transposedSim = logC > 0 && h.dir > 0;
+    if (P.nOps >= kMaxRowOps) {
+      set_error(ctx, kErrUnsupported, "row program too long");
+      return false;
+    }
+    RowOp& o = P.ops[P.nOps++];
+    o.kind = h.kind;
+    o.dir = h.dir;
+    o.diag = -1;
+    if (h.kind != kRowDiag) continue;
+    if (P.nDiag >= kMaxRowDiags) {
+      set_error(ctx, kErrUnsupported, "row program has too many diagonal runs");
+      return false;
+    }
+    std::vector<Term> regTerms, rowTerms, elemTerms;
+    std::vector<int> bits;
+    if (!split_row_diag(ctx, reg, h.terms, &regTerms, &bits, &rowTerms, &elemTerms)) {
+      set_error(ctx, kErrUnsupported, "row program diagonal run does not fit");
+      return false;
+    }
+    RowDiag& D = P.diag[P.nDiag];
+    D.nCtrl = (int)bits.size();
+    for (int c = 0; c < D.nCtrl; ++c) D.ctrlShift[c] = bits[c];
+    D.tab = nullptr;
+    D.permuted = opTransposed ? 1 : 0;
+    if (!regTerms.empty()) {
+      double2* tab = (double2*)arena_alloc(ctx, ((size_t)1 << (q + D.nCtrl)) * sizeof(double2));
+      if (!tab) return false;
+      if (!launch_build_table_ext(ctx, reg, D.nCtrl, bits.data(), regTerms.data(),
+                                  (int)regTerms.size(), tab, D.permuted ? logC : 0))
+        return false;
+      D.tab = tab;
+    }
+    std::vector<Term> left;
+    if (!build_factor_list(ctx, rowTerms, &D.rowF, &left) || !left.empty()) return false;
+    if (!build_factor_list(ctx, elemTerms, &D.elemF, &left) || !left.empty()) return false;
+    D.hasRowF = !factor_empty(D.rowF);
+    D.hasElemF = !factor_empty(D.elemF);
+    o.diag = P.nDiag++;
+  }
+  uint64_t tile = 1ull << lt;
+  uint64_t nCta = ctx->size() / tile;
+  size_t rs = (size_t)((1 << P.logM) + ((1 << P.logM) >> 4));
+  size_t rows = 1ull << P.logRows;
+  size_t smem = rs * rows * ctx->elemBytes + (64 + 128 + 64 + 512) * sizeof(double2) +
+                rows * P.nDiag * (sizeof(double2) + sizeof(int)) + 16;
+  cudaError_t e;
+  {
+    LaunchScope _ls(ctx, kKFft);
+    if (ctx->precision == kC128) {
+      if (logC == 0) e = launch_row_t<double2, 0>(ctx, P, nCta, smem);
+      else if (logC == 1) e = launch_row_t<double2, 1>(ctx, P, nCta, smem);
+      else e = launch_row_t<double2, 2>(ctx, P, nCta, smem);
+    } else {
+      if (logC == 0) e = launch_row_t<float2, 0>(ctx, P, nCta, smem);
+      else if (logC == 1) e = launch_row_t<float2, 1>(ctx, P, nCta, smem);
+      else e = launch_row_t<float2, 2>(ctx, P, nCta, smem);
+    }
+  }
+  if (!cuda_ok(ctx, e, "row program launch")) return false;
+  ctx->cur ^= 1;
+  return true;
+}
+
+}  // namespace cvdv

@@ -70,6 +70,8 @@ SIGNATURES = [
     ("cvdvGetStream", [c_void_p], c_void_p),
     ("cvdvMeasureEach", [c_void_p, POINTER(c_int), c_int, POINTER(c_double)], None),
     ("cvdvLaunchCount", [], ctypes.c_ulonglong),
+    ("cvdvSetFusion", [c_void_p, c_int], None),
+    ("cvdvCancelledTransforms", [c_void_p], ctypes.c_longlong),
     ("cvdvSetTiming", [c_void_p, c_int], None),
     ("cvdvGetKernelStats", [c_void_p, POINTER(c_double), POINTER(ctypes.c_longlong), c_int], c_int),
 ]

@@ -34,7 +34,7 @@ class CudaCvdv:
     (default, the reference's arithmetic) or "complex64" (mixed precision)."""
 
     def __init__(self, numQubits_list: List[int], precision: str = "complex128",
-                 check_errors: bool = False) -> None:
+                 check_errors: bool = False, fusion: bool = True) -> None:
         self._L = _lib.load()
         self.num_registers = len(numQubits_list)
         self.register_dims = [1 << q for q in numQubits_list]
@@ -50,6 +50,12 @@ class CudaCvdv:
         code, msg = _lib.last_error(self.ctx)
         if code:
             raise CvdvError(msg)
+        self.setFusion(fusion)
+
+    def setFusion(self, on: bool) -> None:
+        """(addition) cancel FtP2Q/FtQ2P pairs separated only by gates on other
+        registers (exact identity; on by default)."""
+        self._L.cvdvSetFusion(self.ctx, 1 if on else 0)
 
     def __del__(self):
         try:

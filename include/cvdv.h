@@ -154,6 +154,13 @@ int cvdvPendingStages(CVDVContext* ctx);
 void* cvdvGetStateDevicePtr(CVDVContext* ctx);
 /* The context's CUDA stream (cudaStream_t). */
 void* cvdvGetStream(CVDVContext* ctx);
+/* Queue optimisations.  flags bit 0 (default on): an FtP2Q(r) followed by an
+ * FtQ2P(r) (or the reverse) with only stages that leave register r untouched in
+ * between is removed from the queue -- the pair is the identity, so the result
+ * is unchanged up to rounding.  cvdvCancelledTransforms counts the transforms
+ * removed so far. */
+void cvdvSetFusion(CVDVContext* ctx, int flags);
+long long cvdvCancelledTransforms(CVDVContext* ctx);
 /* Number of kernels this library has launched in the process so far. */
 unsigned long long cvdvLaunchCount(void);
 /* Per-launch timing: when on, every kernel launch of ctx is bracketed by a CUDA

@@ -200,6 +200,36 @@ def test_state_transfer_scaled(n_qubits, mode_qubits):
             np.testing.assert_allclose(sim.m(k), o.m(k), atol=10 * tol)
 
 
+def test_transform_cancellation_matches_unfused():
+    """Queue cancellation of FtP2Q/FtQ2P pairs changes nothing but rounding."""
+    from cvdv_b200 import CudaCvdv, _lib
+    from cvdv_b200 import workloads as W
+    circ = W.state_transfer(n_qubits=4, mode_qubits=12)
+    out = {}
+    for fusion in (True, False):
+        sim = CudaCvdv(circ["qubits"], check_errors=True, fusion=fusion)
+        sim.initStateVector(W.separable_arrays(circ, device="cuda"))
+        W.apply(sim, circ["prep"] + circ["gates"])
+        # displacements in a row on one mode, and a mode gate in between that blocks
+        sim.d(4, 0.3 + 0.1j)
+        sim.d(4, -0.2 + 0.4j)
+        sim.cd(4, 1, 0, 0.25)
+        sim.sheer(4, 0.05)
+        sim.cd(4, 2, 0, -0.15)
+        out[fusion] = (sim.getState(), _lib.load().cvdvCancelledTransforms(sim.ctx))
+    assert out[True][1] > 0 and out[False][1] == 0
+    assert rel(out[True][0], out[False][0]) < 1e-12
+    o = OracleSim(circ["qubits"])
+    o.initStateVector(W.separable_arrays(circ))
+    W.apply(o, circ["prep"] + circ["gates"])
+    o.d(4, 0.3 + 0.1j)
+    o.d(4, -0.2 + 0.4j)
+    o.cd(4, 1, 0, 0.25)
+    o.sheer(4, 0.05)
+    o.cd(4, 2, 0, -0.15)
+    assert rel(out[True][0], o.get_state()) < PLAIN_TOL
+
+
 def test_gaussian_network_scaled():
     from cvdv_b200 import CudaCvdv
     from cvdv_b200 import workloads as W
