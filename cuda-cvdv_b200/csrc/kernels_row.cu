@@ -7,20 +7,25 @@
 // phase kick / next pre-twiddle, inverse DFT, post-twiddle / scale and any
 // following diagonal gates -- runs on a row held on chip.
 //
-// Tiling.  A CTA holds a tile of 4096 (complex128, 256 threads) or 8192
-// (complex64, 512 threads) amplitudes, 16 per thread, in one of two
-// shared-memory buffers (stages read one and write the other).  A register of
-// N <= tile points is processed as tile/N whole rows per CTA.  A longer row is
-// split across a thread-block cluster of C = N / tile CTAs (C = 2 or 4): CTA c
-// holds the contiguous chunk [c M, (c+1) M), M = N / C, and the DFT of the row
-// is one radix-C butterfly across the cluster (operands read from the other
-// CTAs' shared memory, DSMEM) plus an M-point DFT inside each CTA:
+// Tiling.  A CTA of 256 threads holds a tile of 4096 (complex128) or 8192
+// (complex64) amplitudes, 16 or 32 per thread, in one shared-memory buffer;
+// each Stockham stage gathers its operands into registers, synchronises and
+// scatters the results back in place.  Two CTAs fit an SM.  A register of
+// N <= tile points is processed as tile/N whole rows per CTA.  A longer row
+// runs on "big" CTAs of 512 threads (twice the tile, one CTA per SM) and, past
+// that, is split across a thread-block cluster of C = N / tile CTAs (C = 2 or
+// 4): CTA c holds the contiguous chunk [c M, (c+1) M), M = N / C, and the DFT
+// of the row is one radix-C butterfly across the cluster (operands read from
+// the other CTAs' shared memory, DSMEM) plus an M-point DFT inside each CTA:
 //   forward  X[k1 + C k2] = sum_m w_M^{m k2} [ w_N^{m k1} sum_j1 w_C^{j1 k1} x[j1 M + m] ]
 //            -> CTA k1 holds X[k1 + C k2] at local position k2 ("transposed");
 //   inverse  x[j1 M + m]  = sum_k1 w_C^{-j1 k1} w_N^{-m k1} sum_k2 w_M^{-m k2} X[k1 + C k2]
 //            -> consumes the transposed layout and returns the natural one,
-// so FFT . diag . IFFT never reshuffles data between CTAs; a program that ends
-// in the transposed layout is redistributed once before the store.
+// so FFT . diag . IFFT never reshuffles data between CTAs.  A program that
+// starts with an inverse transform loads straight into the transposed layout,
+// and one that ends in it stores from it (CTA k1 writes every C-th element;
+// L2 merges the sectors before they reach HBM).  Diagonal tables applied while
+// the layout is transposed are built permuted to match.
 //
 // The M-point DFT runs as Stockham stages of radix 16 (plus one radix-2/4/8
 // stage when log2 M is not a multiple of 4).  Twiddles come from two small
@@ -42,13 +47,11 @@ constexpr int kRowMinLogN = 8;  // shorter registers use the pass kernels
 
 template <typename C> struct RowCfg;
 template <> struct RowCfg<double2> {
-  static constexpr int LOGT = 8;  // 256 threads x 16 amplitudes (tile 4096)
-  static constexpr int LOGE = 4;
+  static constexpr int LOGE = 4;  // 16 amplitudes per thread
   static constexpr int E = 16;
 };
 template <> struct RowCfg<float2> {
-  static constexpr int LOGT = 8;  // 256 threads x 32 amplitudes (tile 8192)
-  static constexpr int LOGE = 5;
+  static constexpr int LOGE = 5;  // 32 amplitudes per thread
   static constexpr int E = 32;
 };
 
@@ -75,6 +78,7 @@ struct RowProgram {
   int nOps;
   int nDiag;
   int logTwN;
+  int loadT;    // cluster rows: load (and start) in the transposed layout
   const double2* tw;
   RowOp ops[kMaxRowOps];
   RowDiag diag[kMaxRowDiags];
@@ -208,10 +212,10 @@ __device__ __forceinline__ C tw2(const double2* lo, const double2* hi, int e) {
 // One Stockham stage of radix RHO, in place on the single tile buffer: every
 // thread gathers its butterflies' operands into registers, the CTA syncs, and
 // the results are scattered to their autosorted positions.
-template <typename C, int DIR, int RHO>
+template <typename C, int DIR, int RHO, int LOGT>
 __device__ __forceinline__ void row_stage(C* sm, int RS, int logM, int logNs, const TwTables& T) {
   constexpr int LOGRHO = RHO == 16 ? 4 : (RHO == 8 ? 3 : (RHO == 4 ? 2 : 1));
-  constexpr int NT = 1 << RowCfg<C>::LOGT;
+  constexpr int NT = 1 << LOGT;
   constexpr int K = RowCfg<C>::E / RHO;  // butterflies per thread
   const int logNbf = logM - LOGRHO;
   const int ns = 1 << logNs;
@@ -253,38 +257,52 @@ __device__ __forceinline__ void row_stage(C* sm, int RS, int logM, int logNs, co
 }
 
 // M-point DFT of every row segment of the tile
-template <typename C, int DIR>
+template <typename C, int DIR, int LOGT>
 __device__ void local_fft(C* sm, int RS, int logM, const TwTables& T) {
   int logNs = 0, rem = logM;
   while (rem >= 4) {
-    row_stage<C, DIR, 16>(sm, RS, logM, logNs, T);
+    row_stage<C, DIR, 16, LOGT>(sm, RS, logM, logNs, T);
     logNs += 4;
     rem -= 4;
   }
-  if (rem == 3) row_stage<C, DIR, 8>(sm, RS, logM, logNs, T);
-  else if (rem == 2) row_stage<C, DIR, 4>(sm, RS, logM, logNs, T);
-  else if (rem == 1) row_stage<C, DIR, 2>(sm, RS, logM, logNs, T);
+  if (rem == 3) row_stage<C, DIR, 8, LOGT>(sm, RS, logM, logNs, T);
+  else if (rem == 2) row_stage<C, DIR, 4, LOGT>(sm, RS, logM, logNs, T);
+  else if (rem == 1) row_stage<C, DIR, 2, LOGT>(sm, RS, logM, logNs, T);
 }
 
 // ---------------------------------------------------------------- cross-CTA steps
-// Each step reads the cluster peers' tiles (DSMEM) into registers, waits until
-// every CTA has read, then overwrites its own tile.
+// Each cross-CTA step reads the cluster peers' tiles (DSMEM) and overwrites its
+// own tile in place, in two halves: all CTAs read half 0, sync, write half 0,
+// read half 1 (disjoint positions), sync, write half 1.  Holding only half of a
+// thread's outputs keeps the step within 128 registers.
+template <typename C, int LOGC, int LOGT, typename F>
+__device__ __forceinline__ void cluster_exchange(C* sm, F f) {
+  constexpr int NT = 1 << LOGT;
+  constexpr int H = RowCfg<C>::E / 2;
+  cg::cluster_group cl = cg::this_cluster();
+  cl.sync();  // every tile of the cluster is complete
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    C y[H];
+#pragma unroll
+    for (int k = 0; k < H; ++k) y[k] = f(threadIdx.x + (h * H + k) * NT);
+    cl.sync();  // every CTA has read these positions
+#pragma unroll
+    for (int k = 0; k < H; ++k) sm[rpad<C>(threadIdx.x + (h * H + k) * NT)] = y[k];
+  }
+  __syncthreads();
+}
+
 // forward DIF radix-C butterfly: this CTA produces output k1 = rank at every m
-template <typename C, int LOGC>
+template <typename C, int LOGC, int LOGT>
 __device__ void cross_forward(C* sm, const TwTables& T) {
   constexpr int NC = 1 << LOGC;
-  constexpr int NT = 1 << RowCfg<C>::LOGT;
-  constexpr int E = RowCfg<C>::E;
   cg::cluster_group cl = cg::this_cluster();
   const int rank = (int)cl.block_rank();
-  cl.sync();  // every chunk of the row is complete
   const C* peer[NC];
 #pragma unroll
   for (int j = 0; j < NC; ++j) peer[j] = cl.map_shared_rank(sm, j);
-  C y[E];
-#pragma unroll
-  for (int k = 0; k < E; ++k) {
-    int m = threadIdx.x + k * NT;
+  cluster_exchange<C, LOGC, LOGT>(sm, [=](int m) -> C {
     int p = rpad<C>(m);
     C x[NC];
 #pragma unroll
@@ -298,31 +316,20 @@ __device__ void cross_forward(C* sm, const TwTables& T) {
       acc = rank == 0 ? cadd(s02, s13) : rank == 1 ? cadd(d02, d13) : rank == 2 ? csub(s02, s13) : csub(d02, d13);
     }
     int e = m * rank;  // w_N^{m rank}
-    y[k] = e ? cmul(acc, tw2<C, 1>(T.loN, T.hiN, e)) : acc;
-    if ((k & 7) == 7) asm volatile("" ::: "memory");  // bound the loads in flight
-  }
-  cl.sync();  // all reads of every tile are done
-#pragma unroll
-  for (int k = 0; k < E; ++k) sm[rpad<C>(threadIdx.x + k * NT)] = y[k];
-  __syncthreads();
+    return e ? cmul(acc, tw2<C, 1>(T.loN, T.hiN, e)) : acc;
+  });
 }
 
 // inverse DIT radix-C butterfly: this CTA (rank = j1) produces x[j1 M + m]
-template <typename C, int LOGC>
+template <typename C, int LOGC, int LOGT>
 __device__ void cross_inverse(C* sm, const TwTables& T) {
   constexpr int NC = 1 << LOGC;
-  constexpr int NT = 1 << RowCfg<C>::LOGT;
-  constexpr int E = RowCfg<C>::E;
   cg::cluster_group cl = cg::this_cluster();
   const int rank = (int)cl.block_rank();
-  cl.sync();
   const C* peer[NC];
 #pragma unroll
   for (int j = 0; j < NC; ++j) peer[j] = cl.map_shared_rank(sm, j);
-  C y[E];
-#pragma unroll
-  for (int k = 0; k < E; ++k) {
-    int m = threadIdx.x + k * NT;
+  cluster_exchange<C, LOGC, LOGT>(sm, [=](int m) -> C {
     int p = rpad<C>(m);
     C z[NC];
     z[0] = peer[0][p];
@@ -341,20 +348,17 @@ __device__ void cross_inverse(C* sm, const TwTables& T) {
       C s13 = cadd(z[1], z[3]), d13 = rot_mi<C, -1>(csub(z[1], z[3]));
       acc = rank == 0 ? cadd(s02, s13) : rank == 1 ? cadd(d02, d13) : rank == 2 ? csub(s02, s13) : csub(d02, d13);
     }
-    y[k] = acc;
-    if ((k & 7) == 7) asm volatile("" ::: "memory");  // bound the loads in flight
-  }
-  cl.sync();
-#pragma unroll
-  for (int k = 0; k < E; ++k) sm[rpad<C>(threadIdx.x + k * NT)] = y[k];
-  __syncthreads();
+    return acc;
+  });
 }
 
 // layout change: natural (CTA j1 holds k = j1 M + m) <-> transposed (CTA k1 holds k = k1 + C m)
-template <typename C, int LOGC>
+template <typename C, int LOGC, int LOGT>
 __device__ void redistribute(C* sm, int logM, bool toNatural) {
+  // Unlike the butterflies, output position m reads a different position of a
+  // sibling, so every read must finish before any CTA writes: one full round.
   constexpr int NC = 1 << LOGC;
-  constexpr int NT = 1 << RowCfg<C>::LOGT;
+  constexpr int NT = 1 << LOGT;
   constexpr int E = RowCfg<C>::E;
   cg::cluster_group cl = cg::this_cluster();
   const int rank = (int)cl.block_rank();
@@ -374,7 +378,6 @@ __device__ void redistribute(C* sm, int logM, bool toNatural) {
       srcPos = kk & ((1 << logM) - 1);
     }
     y[k] = cl.map_shared_rank(sm, srcRank)[rpad<C>(srcPos)];
-    if ((k & 7) == 7) asm volatile("" ::: "memory");  // bound the loads in flight
   }
   cl.sync();
 #pragma unroll
@@ -385,10 +388,9 @@ __device__ void redistribute(C* sm, int logM, bool toNatural) {
 // ---------------------------------------------------------------- the kernel
 // Single-CTA rows run two CTAs per SM (one loads while the other computes);
 // cluster rows hold the cross-step operands in registers and get the full file.
-template <typename C, int LOGC>
-__global__ void __launch_bounds__(1 << RowCfg<C>::LOGT, LOGC > 0 ? 1 : 2)
+template <typename C, int LOGC, int LOGT>
+__global__ void __launch_bounds__(1 << LOGT, (LOGC > 0 || LOGT > 8) ? 1 : 2)
     k_row(const C* __restrict__ in, C* __restrict__ out, const __grid_constant__ RowProgram P) {
-  constexpr int LOGT = RowCfg<C>::LOGT;
   constexpr int NT = 1 << LOGT;
   constexpr int E = RowCfg<C>::E;
   constexpr int TILE = NT * E;
@@ -417,7 +419,6 @@ __global__ void __launch_bounds__(1 << RowCfg<C>::LOGT, LOGC > 0 ? 1 : 2)
   }
   const uint64_t chunk = base + ((uint64_t)rank << logM);  // first element held here
 
-  const bool headDiag = P.nOps > 0 && P.ops[0].kind == kRowDiag;
   const bool tailDiag = P.nOps > 1 && P.ops[P.nOps - 1].kind == kRowDiag;
   const int opEnd = tailDiag ? P.nOps - 1 : P.nOps;
 
@@ -444,7 +445,10 @@ __global__ void __launch_bounds__(1 << RowCfg<C>::LOGT, LOGC > 0 ? 1 : 2)
   }
   __syncthreads();
 
-  bool transposed = false;
+  // A program whose first transform is inverse loads the row straight into the
+  // transposed layout (stride-C reads; siblings share the sectors through L2).
+  bool transposed = LOGC > 0 && P.loadT;
+  auto gaddrT = [&](int e) -> uint64_t { return base + (uint64_t)rank + ((uint64_t)e << LOGC); };
   // table entry of diag d for tile element (row, m): the table of an op that
   // runs in the transposed layout is stored permuted, so every read is contiguous
   auto tab_at = [&](int d, int row, int m) -> double2 {
@@ -467,7 +471,10 @@ __global__ void __launch_bounds__(1 << RowCfg<C>::LOGT, LOGC > 0 ? 1 : 2)
   {
     C v[E];
 #pragma unroll
-    for (int k = 0; k < E; ++k) v[k] = in[chunk + threadIdx.x + k * NT];
+    for (int k = 0; k < E; ++k) {
+      int e = threadIdx.x + k * NT;
+      v[k] = in[transposed ? gaddrT(e) : chunk + e];
+    }
 #pragma unroll
     for (int k = 0; k < E; ++k) {
       int e = threadIdx.x + k * NT;
@@ -498,33 +505,29 @@ __global__ void __launch_bounds__(1 << RowCfg<C>::LOGT, LOGC > 0 ? 1 : 2)
       __syncthreads();
     } else if (op.dir > 0) {
       if constexpr (LOGC > 0) {
-        if (transposed) redistribute<C, LOGC>(sm, logM, true);
-        cross_forward<C, LOGC>(sm, T);
+        if (transposed) redistribute<C, LOGC, LOGT>(sm, logM, true);
+        cross_forward<C, LOGC, LOGT>(sm, T);
         transposed = true;
       }
-      local_fft<C, 1>(sm, RS, logM, T);
+      local_fft<C, 1, LOGT>(sm, RS, logM, T);
     } else {
       if constexpr (LOGC > 0) {
         if (!transposed) {
-          redistribute<C, LOGC>(sm, logM, false);
+          redistribute<C, LOGC, LOGT>(sm, logM, false);
           transposed = true;
         }
       }
-      local_fft<C, -1>(sm, RS, logM, T);
+      local_fft<C, -1, LOGT>(sm, RS, logM, T);
       if constexpr (LOGC > 0) {
-        cross_inverse<C, LOGC>(sm, T);
+        cross_inverse<C, LOGC, LOGT>(sm, T);
         transposed = false;
       }
     }
   }
-  if constexpr (LOGC > 0) {
-    if (transposed) {
-      redistribute<C, LOGC>(sm, logM, true);
-      transposed = false;
-    }
-  }
-
-  // ---- store (trailing diagonal run applied on the way out)
+  // ---- store (trailing diagonal run applied on the way out).  A row that ends
+  // transposed is written in place with stride C: the sectors this CTA leaves
+  // half-written are completed by its cluster siblings in L2.
+  const bool storeT = LOGC > 0 && transposed;
   if (tailDiag) {
     const int dd = P.ops[P.nOps - 1].diag;
 #pragma unroll 1
@@ -539,14 +542,14 @@ __global__ void __launch_bounds__(1 << RowCfg<C>::LOGT, LOGC > 0 ? 1 : 2)
       for (int k = 0; k < 8; ++k) {
         int e = threadIdx.x + (k0 + k) * NT;
         int row = e >> logM, m = e & (M - 1);
-        out[chunk + e] = cmul(sm[row * RS + rpad<C>(m)], factor_with(dd, row, m, t[k]));
+        out[storeT ? gaddrT(e) : chunk + e] = cmul(sm[row * RS + rpad<C>(m)], factor_with(dd, row, m, t[k]));
       }
     }
   } else {
 #pragma unroll
     for (int k = 0; k < E; ++k) {
       int e = threadIdx.x + k * NT;
-      out[chunk + e] = sm[(e >> logM) * RS + rpad<C>(e & (M - 1))];
+      out[storeT ? gaddrT(e) : chunk + e] = sm[(e >> logM) * RS + rpad<C>(e & (M - 1))];
     }
   }
   if constexpr (LOGC > 0) cg::this_cluster().sync();  // no CTA leaves while peers may read it
@@ -559,8 +562,8 @@ bool row_eligible(Context* ctx, int reg) {
   if (ctx->flw[reg] != 0) return false;
   int lt = row_log_tile(ctx->precision);
   int q = ctx->q[reg];
-  if (q > lt + 2 || q < kRowMinLogN) return false;
-  if (ctx->totalQbt < lt) return false;  // tile larger than the state
+  if (q > lt + 3 || q < kRowMinLogN) return false;  // big tile x cluster of 4 at most
+  if (ctx->totalQbt < lt) return false;            // tile larger than the state
   return true;
 }
 
@@ -633,14 +636,14 @@ bool row_diag_fits(Context* ctx, int reg, const std::vector<Term>& terms) {
   return split_row_diag(ctx, reg, terms, &a, &bits, &b, &c);
 }
 
-template <typename C, int LOGC>
+template <typename C, int LOGC, int LOGT>
 static cudaError_t launch_row_t(Context* ctx, const RowProgram& P, uint64_t nCta, size_t smem) {
-  auto kern = k_row<C, LOGC>;
+  auto kern = k_row<C, LOGC, LOGT>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3((unsigned)nCta);
-  cfg.blockDim = dim3(1u << RowCfg<C>::LOGT);
+  cfg.blockDim = dim3(1u << LOGT);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = ctx->stream;
   cudaLaunchAttribute attr[1];
@@ -655,8 +658,12 @@ static cudaError_t launch_row_t(Context* ctx, const RowProgram& P, uint64_t nCta
 
 bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops) {
   RowProgram P{};
-  int lt = row_log_tile(ctx->precision);
+  // Registers up to the normal tile run two 256-thread CTAs per SM; longer ones
+  // use the big tile (512 threads, twice the amplitudes, one CTA per SM) and, past
+  // that, a cluster of 2 or 4 big tiles.
   int q = ctx->q[reg];
+  int logT = q <= row_log_tile(ctx->precision) ? 8 : 9;
+  int lt = row_log_tile(ctx->precision) + (logT - 8);
   int logC = q > lt ? q - lt : 0;
   P.logN = q;
   P.logM = q - logC;
@@ -664,15 +671,20 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
   P.logTwN = 0;
   while ((1 << P.logTwN) < ctx->twN) ++P.logTwN;
   P.tw = ctx->twiddle;
-  // layout at every op: a forward FFT leaves the cluster transposed, an inverse
-  // natural; the head diag runs at load and the tail diag after the final
-  // redistribution, both natural
-  bool transposedSim = false;
-  int opIndex = -1;
+  // Layout at every op, as the kernel will see it: a program whose first
+  // transform is inverse starts transposed; a forward transform leaves the
+  // cluster transposed, an inverse natural; the tail runs in the final layout.
+  P.loadT = 0;
+  if (logC > 0) {
+    for (const HostRowOp& h : ops)
+      if (h.kind == kRowFft) {
+        P.loadT = h.dir < 0 ? 1 : 0;
+        break;
+      }
+  }
+  bool transposedSim = P.loadT != 0;
   for (const HostRowOp& h : ops) {
-    ++opIndex;
-    bool isHead = opIndex == 0, isTail = opIndex + 1 == (int)ops.size() && opIndex > 0;
-    bool opTransposed = logC > 0 && transposedSim && !isHead && !isTail;
+    bool opTransposed = logC > 0 && transposedSim;
     if (h.kind == kRowFft) transposedSim = logC > 0 && h.dir > 0;
     if (P.nOps >= kMaxRowOps) {
       set_error(ctx, kErrUnsupported, "row program too long");
@@ -723,13 +735,15 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
   {
     LaunchScope _ls(ctx, kKFft);
     if (ctx->precision == kC128) {
-      if (logC == 0) e = launch_row_t<double2, 0>(ctx, P, nCta, smem);
-      else if (logC == 1) e = launch_row_t<double2, 1>(ctx, P, nCta, smem);
-      else e = launch_row_t<double2, 2>(ctx, P, nCta, smem);
+      if (logT == 8) e = launch_row_t<double2, 0, 8>(ctx, P, nCta, smem);
+      else if (logC == 0) e = launch_row_t<double2, 0, 9>(ctx, P, nCta, smem);
+      else if (logC == 1) e = launch_row_t<double2, 1, 9>(ctx, P, nCta, smem);
+      else e = launch_row_t<double2, 2, 9>(ctx, P, nCta, smem);
     } else {
-      if (logC == 0) e = launch_row_t<float2, 0>(ctx, P, nCta, smem);
-      else if (logC == 1) e = launch_row_t<float2, 1>(ctx, P, nCta, smem);
-      else e = launch_row_t<float2, 2>(ctx, P, nCta, smem);
+      if (logT == 8) e = launch_row_t<float2, 0, 8>(ctx, P, nCta, smem);
+      else if (logC == 0) e = launch_row_t<float2, 0, 9>(ctx, P, nCta, smem);
+      else if (logC == 1) e = launch_row_t<float2, 1, 9>(ctx, P, nCta, smem);
+      else e = launch_row_t<float2, 2, 9>(ctx, P, nCta, smem);
     }
   }
   if (!cuda_ok(ctx, e, "row program launch")) return false;
