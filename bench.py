@@ -251,7 +251,7 @@ def run_gpu(args, world, rank, local):
     # algorithmic bytes of a launch are 2 * 2^n * 16 B (complex128).
     alg_bytes = 2 * n_amp * 16
     KNAME = {"pair": "k_pair (H with the neighbouring diagonal runs: conditional phase in p, Rz)",
-             "fft_pass": "k_row (row program: mode DFT + diagonal runs, cluster of 4 CTAs)"}
+             "fft_pass": "k_row (row program: mode DFT + diagonal runs; 2^14-point rows on a 2-CTA cluster of 512-thread CTAs)"}
 
     def kern_roof(st, nbytes):
         out = {}
