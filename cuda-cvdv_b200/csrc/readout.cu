@@ -9,6 +9,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 #include "../../include/cvdv.h"
 #include "cvdv_internal.cuh"
@@ -545,3 +546,163 @@ void cvdvClearError(CVDVContext* ctx) {
 }
 
 }  // extern "C"
+
+// ====================================================================== marginal without allocation
+// Some callers cannot let a library call cudaMalloc: an application whose
+// device memory is owned by another allocator (a framework's caching pool
+// that has reserved the GPU, so a plain cudaMalloc fails although the pool has
+// room), a service that sizes its device memory once at start-up and must not
+// grow it afterwards, or a loop that cannot afford the device-wide
+// synchronisation that cudaMalloc and cudaFree may perform.  For them,
+// cvdvMeasureMultipleNoAlloc computes the same joint marginal as
+// cvdvMeasureMultiple on a state they own, writes it to an output they own,
+// and keeps its per-block partial histograms in the fixed array below.
+//
+// The array is part of this library's device code: every GPU that loads the
+// library holds it (kNoAllocBlocks x kNoAllocMaxBins doubles = 4.625 MiB) until
+// the process exits.  Every call shares it and it keeps the last call's
+// contents; nothing in it has to start at zero, because each block writes its
+// whole histogram row before the final kernel reads it.  Calls whose kernels
+// overlap on the GPU (different streams, no ordering between them) race on it.
+namespace cvdv {
+
+constexpr int kNoAllocBlocks = 148;
+constexpr int kNoAllocMaxBins = 4096;  // 2^12: joint marginals of up to 12 qubits
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) double g_noAllocScratch[kNoAllocBlocks * kNoAllocMaxBins];
+
+static std::mutex g_noAllocMu;
+static double* g_noAllocPtr[kNoAllocMaxDevices];  // device address per device, set up on first use
+
+// Device address of the scratch array on the current device.  The array's name
+// in host code is only a handle for the runtime; the address the kernels use is
+// looked up once per device, with that device current.
+static double* no_alloc_scratch(int dev) {
+  std::lock_guard<std::mutex> lk(g_noAllocMu);
+  if (!g_noAllocPtr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noAllocScratch);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      set_error(nullptr, kErrCuda, "cvdvMeasureMultipleNoAlloc: scratch lookup on device %d: %s", dev,
+                cudaGetErrorString(e));
+      return nullptr;
+    }
+    g_noAllocPtr[dev] = (double*)p;
+  }
+  return g_noAllocPtr[dev];
+}
+
+static bool device_pointer_on(const void* p, int dev) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) && a.device == dev;
+}
+
+}  // namespace cvdv
+
+extern "C" int cvdvMeasureMultipleNoAlloc(const void* state, int precision, const int* numQubits,
+                                          int numReg, const int* regIdxs, int numRegs, double* probsOut,
+                                          void* stream) {
+  const char* fn = "cvdvMeasureMultipleNoAlloc";
+  if (!state || !probsOut || !numQubits || !regIdxs) {
+    set_error(nullptr, kErrInvalidArg, "%s: null pointer argument", fn);
+    return kErrInvalidArg;
+  }
+  if (precision != kC128 && precision != kC64) {
+    set_error(nullptr, kErrInvalidArg, "%s: precision %d (0 = complex128, 1 = complex64)", fn, precision);
+    return kErrInvalidArg;
+  }
+  if (numReg < 1 || numReg > kMaxRegs) {
+    set_error(nullptr, kErrInvalidArg, "%s: numReg %d outside 1..%d", fn, numReg, kMaxRegs);
+    return kErrInvalidArg;
+  }
+  int flw[kMaxRegs];
+  int total = 0;
+  for (int r = numReg - 1; r >= 0; --r) {
+    if (numQubits[r] < 1 || numQubits[r] > kMaxTotalQubits) {
+      set_error(nullptr, kErrInvalidArg, "%s: register %d has %d qubits", fn, r, numQubits[r]);
+      return kErrInvalidArg;
+    }
+    flw[r] = total;
+    total += numQubits[r];
+  }
+  if (total > kMaxTotalQubits) {
+    set_error(nullptr, kErrInvalidArg, "%s: %d qubits in total exceed %d", fn, total, kMaxTotalQubits);
+    return kErrInvalidArg;
+  }
+  if (numRegs < 1 || numRegs > 16 || numRegs > numReg) {
+    set_error(nullptr, kErrInvalidArg, "%s: numRegs %d outside 1..min(16, numReg)", fn, numRegs);
+    return kErrInvalidArg;
+  }
+  MargDesc D{};
+  D.nSel = numRegs;
+  long long bins = 1;
+  for (int s = 0; s < numRegs; ++s) {
+    int r = regIdxs[s];
+    if (r < 0 || r >= numReg) {
+      set_error(nullptr, kErrInvalidArg, "%s: register index %d outside 0..%d", fn, r, numReg - 1);
+      return kErrInvalidArg;
+    }
+    for (int t = 0; t < s; ++t)
+      if (regIdxs[t] == r) {
+        set_error(nullptr, kErrInvalidArg, "%s: register %d selected twice", fn, r);
+        return kErrInvalidArg;
+      }
+    bins <<= numQubits[r];  // at most 2^12 * 2^34, no overflow
+    if (bins > kNoAllocMaxBins) break;
+    D.shift[s] = flw[r];
+    D.mask[s] = (1 << numQubits[r]) - 1;
+    D.stride[s] = bins >> numQubits[r];  // first selected register fastest, as cvdvMeasureMultiple
+  }
+  if (bins > kNoAllocMaxBins) {
+    set_error(nullptr, kErrInvalidArg,
+              "%s: the selected registers span more than %d outcomes; this entry point holds at most "
+              "%d (12 qubits) -- use cvdvMeasureMultiple for larger marginals",
+              fn, kNoAllocMaxBins, kNoAllocMaxBins);
+    return kErrInvalidArg;
+  }
+  D.outSize = bins;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
+    cudaGetLastError();
+    set_error(nullptr, kErrCuda, "%s: no usable current device", fn);
+    return kErrCuda;
+  }
+  const size_t elem = precision == kC128 ? sizeof(double2) : sizeof(float2);
+  if (((uintptr_t)state % elem) || ((uintptr_t)probsOut % sizeof(double)) ||
+      !device_pointer_on(state, dev) || !device_pointer_on(probsOut, dev)) {
+    set_error(nullptr, kErrInvalidArg,
+              "%s: state and probsOut must be aligned device memory of the current device %d", fn, dev);
+    return kErrInvalidArg;
+  }
+  double* scratch = no_alloc_scratch(dev);
+  if (!scratch) return kErrCuda;
+  cudaStream_t s = (cudaStream_t)stream;
+  const uint64_t n = 1ull << total;
+  uint64_t maxBlocks = (n + 255) / 256;
+  int blocks = kNoAllocBlocks < maxBlocks ? kNoAllocBlocks : (int)maxBlocks;
+  size_t smem = (size_t)bins * sizeof(double);
+  {
+    LaunchScope _ls(nullptr, kKReduce);
+    if (precision == kC128)
+      k_marg_smem<double2><<<blocks, 256, smem, s>>>((const double2*)state, n, D, scratch);
+    else
+      k_marg_smem<float2><<<blocks, 256, smem, s>>>((const float2*)state, n, D, scratch);
+  }
+  {
+    LaunchScope _ls(nullptr, kKReduce);
+    k_marg_final<<<(int)((bins + 255) / 256), 256, 0, s>>>(scratch, blocks, bins, probsOut);
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error(nullptr, kErrCuda, "%s: launch: %s", fn, cudaGetErrorString(e));
+    return kErrCuda;
+  }
+  return kOk;
+}

@@ -69,6 +69,8 @@ SIGNATURES = [
     ("cvdvGetStateDevicePtr", [c_void_p], c_void_p),
     ("cvdvGetStream", [c_void_p], c_void_p),
     ("cvdvMeasureEach", [c_void_p, POINTER(c_int), c_int, POINTER(c_double)], None),
+    ("cvdvMeasureMultipleNoAlloc",
+     [c_void_p, c_int, POINTER(c_int), c_int, POINTER(c_int), c_int, c_void_p, c_void_p], c_int),
     ("cvdvLaunchCount", [], ctypes.c_ulonglong),
     ("cvdvSetFusion", [c_void_p, c_int], None),
     ("cvdvCancelledTransforms", [c_void_p], ctypes.c_longlong),

@@ -173,6 +173,22 @@ int cvdvGetKernelStats(CVDVContext* ctx, double* msOut, long long* countOut, int
 /* Marginals of several single registers in one pass over the state:
  * probsOut receives, for each k, dims[regIdxs[k]] values back to back. */
 void cvdvMeasureEach(CVDVContext* ctx, const int* regIdxs, int numRegs, double* probsOut);
+/* No counterpart in the reference.  The joint marginal of cvdvMeasureMultiple
+ * for callers that cannot let the library allocate device memory (their device
+ * memory belongs to another allocator, is fixed at start-up, or must not see
+ * the device-wide synchronisation of cudaMalloc/cudaFree).  The caller passes
+ * its own state (device memory of the current device, layout numQubits[0..numReg),
+ * precision 0 = complex128 / 1 = complex64), its own device output probsOut of
+ * prod 2^numQubits[regIdxs[k]] doubles, and a cudaStream_t (NULL = default
+ * stream); the call only enqueues work and returns 0 or an error code (message
+ * via cvdvGetLastError(NULL, ...)).  Partial histograms live in a fixed
+ * 4.625 MiB device array that every GPU loading the library holds until exit,
+ * so marginals are limited to 4096 outcomes (12 qubits); larger ones are
+ * rejected.  The first call on a device looks up that array's address and
+ * should come before any stream capture.  All calls share the array: calls
+ * that overlap on the GPU race. */
+int cvdvMeasureMultipleNoAlloc(const void* state, int precision, const int* numQubits, int numReg,
+                               const int* regIdxs, int numRegs, double* probsOut, void* stream);
 
 #ifdef __cplusplus
 }
