@@ -250,12 +250,13 @@ def run_gpu(args, world, rank, local):
     # Every kernel of this workload is one read + write of the state: the
     # algorithmic bytes of a launch are 2 * 2^n * 16 B (complex128).
     alg_bytes = 2 * n_amp * 16
-    KNAME = {"pair": "k_pair (H with the neighbouring diagonal runs: conditional phase in p, Rz)",
+    KNAME = {"seq": "k_seq (qubit-gate sequence: H, conditional phase in p and Rz on up to four qubits per pass)",
+             "pair": "k_pair (one qubit gate with the neighbouring diagonal runs)",
              "fft_pass": "k_row (row program: mode DFT + diagonal runs; 2^14-point rows on a 2-CTA cluster of 512-thread CTAs)"}
 
     def kern_roof(st, nbytes):
         out = {}
-        for k in ("pair", "fft_pass"):
+        for k in ("seq", "pair", "fft_pass"):
             t, n = st[k]
             if n:
                 per = t / n
@@ -321,7 +322,8 @@ def run_gpu(args, world, rank, local):
                 "d2h_bytes_per_step": d2h, "includes": "init from host arrays + 2 prep gates + 42 gates + 14 marginals"},
         "norm_after": norm,
         "queue_fusion": "FtP2Q/FtQ2P pairs separated only by gates on other registers are cancelled "
-                        "(exact identity); see every_transform_executed for the run without it",
+                        "(exact identity) and chains of qubit gates on up to four qubits run as one pass; "
+                        "every_transform_executed is the run with both off (one pass per gate)",
         "every_transform_executed": {"value": G * world / (msnf * 1e-3), "ms_per_step": msnf,
                                      "gpu_launches": int(launchesnf), "kernels": krnf, "norm_after": normnf},
         "mixed_c64": {"value": G * world / (ms64 * 1e-3), "ms_per_step": ms64, "gpu_launches": int(launches64),

@@ -490,6 +490,7 @@ unsigned long long cvdvLaunchCount(void) { return cvdv::g_launches.load(); }
 void cvdvSetFusion(CVDVContext* ctx, int flags) {
   if (!ctx) return;
   C(ctx)->cancelFt = (flags & 1) != 0;
+  C(ctx)->fuseSeq = (flags & 2) != 0;
 }
 
 long long cvdvCancelledTransforms(CVDVContext* ctx) { return ctx ? C(ctx)->ftCancelled * 2 : 0; }

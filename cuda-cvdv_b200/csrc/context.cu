@@ -15,6 +15,8 @@
 #include <map>
 #include <mutex>
 
+#include <algorithm>
+
 #include "cvdv_internal.cuh"
 
 namespace cvdv {
@@ -354,6 +356,34 @@ struct Op {
   std::vector<HostRowOp> row;
 };
 
+// Number of consecutive pair ops from ops[i] that one qubit-gate sequence can
+// take: at most kSeqMaxBits distinct bits, and every diagonal run among them
+// (each pair's `pre`, the last op's `post`) still fitting with the final bit set.
+static size_t seq_extent(Context* ctx, const std::vector<Op>& ops, size_t i) {
+  std::vector<int> bits;
+  int nOps = 0, nDiag = 0;
+  size_t j = i;
+  for (; j < ops.size(); ++j) {
+    const Op& op = ops[j];
+    if (op.rowReg >= 0 || !op.st || op.st->kind != kStPair) break;
+    std::vector<int> nb = bits;
+    if (std::find(nb.begin(), nb.end(), op.st->bit) == nb.end()) nb.push_back(op.st->bit);
+    const int addDiag = (op.pre.empty() ? 0 : 1) + (op.post.empty() ? 0 : 1);
+    if ((int)nb.size() > kSeqMaxBits || nOps + 1 + addDiag > kSeqMaxOps ||
+        nDiag + addDiag > kSeqMaxDiags)
+      break;
+    bool ok = true;
+    for (size_t k = i; k <= j && ok; ++k)
+      ok = (ops[k].pre.empty() || seq_diag_ok(ctx, nb, ops[k].pre)) &&
+           (ops[k].post.empty() || seq_diag_ok(ctx, nb, ops[k].post));
+    if (!ok) break;
+    bits.swap(nb);
+    nOps += 1 + addDiag;
+    nDiag += addDiag;
+  }
+  return j - i;
+}
+
 bool flush(Context* ctx) {
   if (ctx->pending.empty()) return true;
   if (!ctx->initialized) {
@@ -435,7 +465,24 @@ bool flush(Context* ctx) {
       ops.back().post = diag;
     }
   }
-  for (Op& op : ops) {
+  for (size_t oi = 0; oi < ops.size(); ++oi) {
+    Op& op = ops[oi];
+    if (ctx->fuseSeq && op.st && op.st->kind == kStPair) {
+      const size_t ext = seq_extent(ctx, ops, oi);
+      if (ext >= 2) {
+        std::vector<HostSeqOp> seq;
+        for (size_t k = oi; k < oi + ext; ++k) {
+          if (!ops[k].pre.empty()) seq.push_back({1, -1, {}, ops[k].pre});
+          HostSeqOp p{0, ops[k].st->bit, {}, {}};
+          for (int e = 0; e < 4; ++e) p.m[e] = ops[k].st->m[e];
+          seq.push_back(std::move(p));
+          if (!ops[k].post.empty()) seq.push_back({1, -1, {}, ops[k].post});
+        }
+        if (!launch_seq(ctx, seq)) return false;
+        oi += ext - 1;
+        continue;
+      }
+    }
     if (op.rowReg >= 0) {
       if (!launch_row_program(ctx, op.rowReg, op.row)) return false;
       continue;

@@ -203,7 +203,8 @@ enum KernelKind : int {
   kKInit = 5,
   kKReduce = 6,
   kKPhaseSpace = 7,
-  kKindCount = 8,
+  kKSeq = 8,
+  kKindCount = 9,
 };
 
 struct TimingRec {
@@ -257,6 +258,7 @@ struct Context {
   // stages that leave register r untouched in between is the identity; both are
   // dropped from the queue.  On by default (cvdvSetFusion).
   bool cancelFt = true;
+  bool fuseSeq = true;  // run chains of qubit gates as one qubit-gate sequence pass
   int nextFtTag = 1;
   long long ftCancelled = 0;
 
@@ -322,6 +324,21 @@ struct HostRowOp {
 bool row_eligible(Context* ctx, int reg);
 bool row_diag_fits(Context* ctx, int reg, const std::vector<Term>& terms);
 bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops);
+// qubit-gate sequences (kernels_seq.cu): 2x2 gates on up to four bits and the
+// diagonal runs between them in one pass
+constexpr int kSeqMaxBits = 4;
+constexpr int kSeqMaxOps = 24;
+constexpr int kSeqMaxDiags = 10;
+constexpr int kSeqMaxTabs = 4;
+struct HostSeqOp {
+  int kind;  // 0 pair (bit, m), 1 diagonal run (terms)
+  int bit;
+  double2 m[4];
+  std::vector<Term> terms;
+};
+// whether a diagonal run can ride in a sequence over `bits` (global bit positions)
+bool seq_diag_ok(Context* ctx, const std::vector<int>& bits, const std::vector<Term>& terms);
+bool launch_seq(Context* ctx, const std::vector<HostSeqOp>& ops);
 // outer[h] = prod over registers but the last of phi_r[j_r(h)], h < 2^(n - q_last)
 bool launch_outer(Context* ctx, const double2* const* regArrays, double2* outer);
 // FFT of the live state along `reg` into `out` (state untouched); `tmp` is the

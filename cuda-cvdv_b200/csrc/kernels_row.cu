@@ -238,14 +238,20 @@ __device__ __forceinline__ void row_stage(C* sm, int RS, int logM, int logNs, co
     int jb = bf & ((1 << logNbf) - 1);
     int jm = jb & (ns - 1);
     if (jm) {
-      C w1 = tw2<C, DIR>(T.loM, T.hiM, jm << sc);
-      C w = w1;
-      v[k][1] = cmul(v[k][1], w);
+      // powers w^u of the butterfly's base twiddle as a tree of depth log2(RHO):
+      // w^(u + 2^j) = w^u * w^(2^j), so no product waits on more than four others
+      C w[RHO];
+      w[1] = tw2<C, DIR>(T.loM, T.hiM, jm << sc);
 #pragma unroll
-      for (int u = 2; u < RHO; ++u) {
-        w = cmul(w, w1);
-        v[k][u] = cmul(v[k][u], w);
+      for (int p = 1; p < RHO / 2; p <<= 1) {
+        w[2 * p] = cmul(w[p], w[p]);
+#pragma unroll
+        for (int u = 1; u < p; ++u) w[p + u] = cmul(w[p], w[u]);
       }
+#pragma unroll
+      for (int u = RHO / 2 + 1; u < RHO; ++u) w[u] = cmul(w[RHO / 2], w[u - RHO / 2]);
+#pragma unroll
+      for (int u = 1; u < RHO; ++u) v[k][u] = cmul(v[k][u], w[u]);
     }
     bfly<C, DIR, RHO>(v[k]);
     C* out = sm + row * RS;
@@ -555,6 +561,171 @@ __global__ void __launch_bounds__(1 << LOGT, (LOGC > 0 || LOGT > 8) ? 1 : 2)
   if constexpr (LOGC > 0) cg::this_cluster().sync();  // no CTA leaves while peers may read it
 }
 
+// ---------------------------------------------------------------- register-resident rows
+// Rows that fit one CTA (up to 2^13 complex128 / 2^14 complex64 points) run in
+// k_rowr: each thread keeps 16 amplitudes of one row in registers for the whole
+// program -- elements t + TPR v (v = 0..15) of its row, TPR = M / 16 threads per
+// row.  A Stockham stage of radix R gives thread t the butterflies j = t + b TPR
+// (b < 16/R); their inputs j + u M/R are exactly the thread's 16 elements
+// (register b + (16/R) u), and the last stage's outputs land on the same
+// positions.  So the global load, the store and every diagonal run between
+// transforms work on registers in place; only the stages inside a transform
+// exchange data, through one padded shared-memory row.  Row length, radices and
+// strides are template constants, so every shared-memory address is a
+// per-thread base plus an immediate offset.
+
+template <typename C, int DIR, int LOGM, int LOGRAD, int LOGNS>
+__device__ __forceinline__ void rr_butterflies(C (&v)[16], int t, const double2* lo, const double2* hi) {
+  constexpr int RAD = 1 << LOGRAD, NB = 16 / RAD, TPR = 1 << (LOGM - 4);
+#pragma unroll
+  for (int b = 0; b < NB; ++b) {
+    C x[RAD];
+#pragma unroll
+    for (int u = 0; u < RAD; ++u) x[u] = v[b + NB * u];
+    if constexpr (LOGNS > 0) {
+      const int jm = (t + b * TPR) & ((1 << LOGNS) - 1);
+      // w_{ns R}^{jm u} = w_M^{(jm u) << (LOGM - LOGNS - LOGRAD)}; powers as a tree
+      C w[RAD];
+      w[1] = tw2<C, DIR>(lo, hi, jm << (LOGM - LOGNS - LOGRAD));
+#pragma unroll
+      for (int p = 1; p < RAD / 2; p <<= 1) {
+        w[2 * p] = cmul(w[p], w[p]);
+#pragma unroll
+        for (int u = 1; u < p; ++u) w[p + u] = cmul(w[p], w[u]);
+      }
+#pragma unroll
+      for (int u = RAD / 2 + 1; u < RAD; ++u) w[u] = cmul(w[RAD / 2], w[u - RAD / 2]);
+#pragma unroll
+      for (int u = 1; u < RAD; ++u) x[u] = cmul(x[u], w[u]);
+    }
+    bfly<C, DIR, RAD>(x);
+#pragma unroll
+    for (int u = 0; u < RAD; ++u) v[b + NB * u] = x[u];
+  }
+}
+
+// outputs of a stage to their autosorted positions, then the next stage's inputs
+template <typename C, int LOGM, int LOGRAD, int LOGNS>
+__device__ __forceinline__ void rr_exchange(C (&v)[16], C* smrow, int t) {
+  constexpr int RAD = 1 << LOGRAD, NB = 16 / RAD, TPR = 1 << (LOGM - 4);
+#pragma unroll
+  for (int b = 0; b < NB; ++b) {
+    const int j = t + b * TPR;
+    const int y = ((j >> LOGNS) << (LOGNS + LOGRAD)) + (j & ((1 << LOGNS) - 1));
+#pragma unroll
+    for (int u = 0; u < RAD; ++u) smrow[rpad<C>(y + (u << LOGNS))] = v[b + NB * u];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = smrow[rpad<C>(t + k * TPR)];
+  __syncthreads();
+}
+
+template <typename C, int DIR, int LOGM, int S>
+__device__ __forceinline__ void rr_stages(C (&v)[16], C* smrow, int t, const double2* lo, const double2* hi) {
+  constexpr int N16 = LOGM / 4, REM = LOGM % 4;
+  if constexpr (S < N16) {
+    rr_butterflies<C, DIR, LOGM, 4, 4 * S>(v, t, lo, hi);
+    if constexpr (S + 1 < N16 || REM) rr_exchange<C, LOGM, 4, 4 * S>(v, smrow, t);
+    rr_stages<C, DIR, LOGM, S + 1>(v, smrow, t, lo, hi);
+  } else if constexpr (REM > 0) {
+    rr_butterflies<C, DIR, LOGM, REM, 4 * N16>(v, t, lo, hi);
+  }
+}
+
+template <typename C, int LOGM>
+__device__ __forceinline__ void rr_diag(C (&v)[16], const RowDiag& D, uint64_t rowBase, int t) {
+  constexpr int TPR = 1 << (LOGM - 4);
+  const double2 rs = D.hasRowF ? eval_factor(D.rowF, rowBase) : make_double2(1.0, 0.0);
+  if (D.tab) {
+    int seg = 0;
+    for (int c = 0; c < D.nCtrl; ++c) seg |= (int)((rowBase >> D.ctrlShift[c]) & 1ull) << c;
+    const double2* tp = D.tab + ((size_t)seg << LOGM) + t;
+#pragma unroll
+    for (int k0 = 0; k0 < 16; k0 += 8) {
+      double2 w[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) w[k] = __ldg(tp + (k0 + k) * TPR);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        if (D.hasRowF) w[k] = dmul(w[k], rs);
+        v[k0 + k] = cmul(v[k0 + k], fromd<C>(w[k]));
+      }
+    }
+  } else if (D.hasRowF) {
+    const C c = fromd<C>(rs);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) v[k] = cmul(v[k], c);
+  }
+}
+
+// 256-thread CTAs run two per SM; 512- and 1024-thread CTAs one
+template <typename C, int LOGM, int LOGR>
+__global__ void __launch_bounds__(1 << (LOGM - 4 + LOGR), (LOGM - 4 + LOGR) > 8 ? 1 : 2)
+    k_rowr(const C* __restrict__ in, C* __restrict__ out, const __grid_constant__ RowProgram P) {
+  constexpr int M = 1 << LOGM, TPR = M >> 4, NT = TPR << LOGR, RS = M + (M >> 4);
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* sm = reinterpret_cast<C*>(smraw);
+  double2* lo = reinterpret_cast<double2*>(sm + (RS << LOGR));  // w_M^e, e < 64
+  double2* hi = lo + 64;                                         // w_M^(64 h), h < M / 64
+  const int tid = threadIdx.x;
+  const int row = tid >> (LOGM - 4);
+  const int t = tid & (TPR - 1);
+  C* smrow = sm + row * RS;
+  const uint64_t rowBase = ((uint64_t)blockIdx.x << (LOGM + LOGR)) + ((uint64_t)row << LOGM);
+
+  const int scM = P.logTwN - LOGM;
+  for (int i = tid; i < 64 + (M >> 6); i += NT) {
+    const int e = i < 64 ? i : (i - 64) << 6;
+    lo[i] = __ldg(P.tw + ((size_t)e << scM));  // lo and hi are one array
+  }
+  C v[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = in[rowBase + t + k * TPR];
+  __syncthreads();
+
+  for (int o = 0; o < P.nOps; ++o) {
+    const RowOp& op = P.ops[o];
+    if (op.kind == kRowDiag) rr_diag<C, LOGM>(v, P.diag[op.diag], rowBase, t);
+    else if (op.dir > 0) rr_stages<C, 1, LOGM, 0>(v, smrow, t, lo, hi);
+    else rr_stages<C, -1, LOGM, 0>(v, smrow, t, lo, hi);
+  }
+#pragma unroll
+  for (int k = 0; k < 16; ++k) out[rowBase + t + k * TPR] = v[k];
+}
+
+// largest row k_rowr takes (one CTA: 16 amplitudes x 512 / 1024 threads)
+static int rowr_max_log(int precision) { return precision == kC128 ? 13 : 14; }
+
+template <typename C, int LOGM>
+static cudaError_t launch_rowr_t(Context* ctx, const RowProgram& P) {
+  constexpr int LOGR = LOGM < 12 ? 12 - LOGM : 0;
+  constexpr int NT = 1 << (LOGM - 4 + LOGR);
+  constexpr int M = 1 << LOGM;
+  const size_t smem = (size_t)(M + (M >> 4)) * (1 << LOGR) * sizeof(C) + (64 + (M >> 6)) * sizeof(double2);
+  auto kern = k_rowr<C, LOGM, LOGR>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const uint64_t nCta = ctx->size() >> (LOGM + LOGR);
+  kern<<<(unsigned)nCta, NT, smem, ctx->stream>>>((const C*)ctx->state(), (C*)ctx->other(), P);
+  return cudaGetLastError();
+}
+
+template <typename C>
+static cudaError_t launch_rowr(Context* ctx, const RowProgram& P, int q) {
+  switch (q) {
+    case 8: return launch_rowr_t<C, 8>(ctx, P);
+    case 9: return launch_rowr_t<C, 9>(ctx, P);
+    case 10: return launch_rowr_t<C, 10>(ctx, P);
+    case 11: return launch_rowr_t<C, 11>(ctx, P);
+    case 12: return launch_rowr_t<C, 12>(ctx, P);
+    case 13: return launch_rowr_t<C, 13>(ctx, P);
+    default:
+      if constexpr (sizeof(C) == sizeof(float2)) return launch_rowr_t<C, 14>(ctx, P);
+      return cudaErrorInvalidValue;
+  }
+}
+
 // ---------------------------------------------------------------- host side
 int row_log_tile(int precision) { return precision == kC128 ? 12 : 13; }
 
@@ -724,6 +895,18 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
     D.hasRowF = !factor_empty(D.rowF);
     D.hasElemF = !factor_empty(D.elemF);
     o.diag = P.nDiag++;
+  }
+  bool elemF = false;
+  for (int d = 0; d < P.nDiag; ++d) elemF |= P.diag[d].hasElemF != 0;
+  if (logC == 0 && !elemF && q <= rowr_max_log(ctx->precision)) {
+    cudaError_t er;
+    {
+      LaunchScope _ls(ctx, kKFft);
+      er = ctx->precision == kC128 ? launch_rowr<double2>(ctx, P, q) : launch_rowr<float2>(ctx, P, q);
+    }
+    if (!cuda_ok(ctx, er, "row program launch")) return false;
+    ctx->cur ^= 1;
+    return true;
   }
   uint64_t tile = 1ull << lt;
   uint64_t nCta = ctx->size() / tile;

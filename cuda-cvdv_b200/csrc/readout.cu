@@ -228,6 +228,141 @@ __global__ void __launch_bounds__(256) k_marg_global(const C* __restrict__ st, u
   }
 }
 
+// Tiled marginals: several outputs (each the joint marginal of some registers) in
+// one pass.  A block reads tiles of 256 x 16 consecutive amplitudes.  An output
+// whose registers all lie above the tile's 12 index bits has one bin per tile:
+// the block sums the tile once and thread 0 adds it (no atomics at all, which
+// is the case for every qubit register of a mode-last layout).  Other outputs
+// bin each amplitude with warp-aggregated shared atomics.
+constexpr int kMargLogV = 4;
+constexpr int kMargLogTile = 8 + kMargLogV;
+constexpr int kMargMaxOut = 16;
+constexpr int kMargSmemBins = 4096;
+
+struct MargOut {
+  int nSel, sel0, off, high;
+};
+struct MargPlan {
+  int nOut, nHigh, totalBins;
+  int shift[16], mask[16], stride[16];
+  MargOut out[kMargMaxOut];
+};
+
+__device__ __forceinline__ int marg_out_bin(const MargPlan& P, const MargOut& O, uint64_t i) {
+  int b = 0;
+  for (int s = 0; s < O.nSel; ++s)
+    b += (int)((i >> P.shift[O.sel0 + s]) & (uint64_t)P.mask[O.sel0 + s]) * P.stride[O.sel0 + s];
+  return b;
+}
+
+template <typename C>
+__global__ void __launch_bounds__(256) k_marg_tiles(const C* __restrict__ st, uint64_t nTiles,
+                                                   const __grid_constant__ MargPlan P,
+                                                   double* __restrict__ part) {
+  constexpr int V = 1 << kMargLogV;
+  extern __shared__ double hist[];
+  __shared__ double red[8];
+  for (int b = threadIdx.x; b < P.totalBins; b += blockDim.x) hist[b] = 0.0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (uint64_t tile = blockIdx.x; tile < nTiles; tile += gridDim.x) {
+    const uint64_t t0 = tile << kMargLogTile;
+    double p[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const double2 a = tod<C>(st[t0 + threadIdx.x + (v << 8)]);
+      p[v] = a.x * a.x + a.y * a.y;
+    }
+    if (P.nHigh < P.nOut) {
+      for (int o = 0; o < P.nOut; ++o) {
+        const MargOut& O = P.out[o];
+        if (O.high) continue;
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          const int bin = marg_out_bin(P, O, t0 + threadIdx.x + (v << 8));
+          const int b0 = __shfl_sync(0xffffffffu, bin, 0);
+          if (__all_sync(0xffffffffu, bin == b0)) {
+            double q = p[v];
+#pragma unroll
+            for (int d = 16; d > 0; d >>= 1) q += __shfl_down_sync(0xffffffffu, q, d);
+            if (lane == 0) atomicAdd(&hist[O.off + b0], q);
+          } else {
+            atomicAdd(&hist[O.off + bin], p[v]);
+          }
+        }
+      }
+    }
+    if (P.nHigh) {
+      double q = 0.0;
+#pragma unroll
+      for (int v = 0; v < V; ++v) q += p[v];
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1) q += __shfl_down_sync(0xffffffffu, q, d);
+      if (lane == 0) red[warp] = q;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double S = 0.0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) S += red[w];
+        for (int o = 0; o < P.nOut; ++o)
+          if (P.out[o].high) hist[P.out[o].off + marg_out_bin(P, P.out[o], t0)] += S;
+      }
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < P.totalBins; b += blockDim.x)
+    part[(size_t)blockIdx.x * P.totalBins + b] = hist[b];
+}
+
+// One pass for `outs` (each a list of registers, first fastest); every output
+// must have at most kMargSmemBins bins in total and the state at least one tile.
+// dOut receives the outputs back to back.
+static bool marginals_tiled(Context* ctx, const std::vector<std::vector<int>>& outs, double* dOut) {
+  MargPlan P{};
+  int sel = 0;
+  for (const auto& regs : outs) {
+    MargOut& O = P.out[P.nOut++];
+    O.nSel = (int)regs.size();
+    O.sel0 = sel;
+    O.off = P.totalBins;
+    O.high = 1;
+    int stride = 1;
+    for (int r : regs) {
+      P.shift[sel] = ctx->flw[r];
+      P.mask[sel] = (1 << ctx->q[r]) - 1;
+      P.stride[sel] = stride;
+      stride <<= ctx->q[r];
+      if (ctx->flw[r] < kMargLogTile) O.high = 0;
+      ++sel;
+    }
+    P.nHigh += O.high;
+    P.totalBins += stride;
+  }
+  const uint64_t nTiles = ctx->size() >> kMargLogTile;
+  uint64_t blocks = P.totalBins <= 256 ? 148ull * 4 : 148ull * 2;
+  if (blocks > nTiles) blocks = nTiles;
+  double* part = (double*)arena_alloc(ctx, (size_t)blocks * P.totalBins * sizeof(double));
+  if (!part) return false;
+  const size_t smem = (size_t)P.totalBins * sizeof(double);
+  {
+    LaunchScope _ls(ctx, kKReduce);
+    if (ctx->precision == kC128)
+      k_marg_tiles<double2><<<(unsigned)blocks, 256, smem, ctx->stream>>>((const double2*)ctx->state(), nTiles, P, part);
+    else
+      k_marg_tiles<float2><<<(unsigned)blocks, 256, smem, ctx->stream>>>((const float2*)ctx->state(), nTiles, P, part);
+  }
+  {
+    LaunchScope _ls(ctx, kKReduce);
+    k_marg_final<<<(P.totalBins + 255) / 256, 256, 0, ctx->stream>>>(part, (int)blocks, P.totalBins, dOut);
+  }
+  return cuda_ok(ctx, cudaGetLastError(), "marginal launch");
+}
+
+static bool tiled_ok(Context* ctx, long long bins) {
+  return bins <= kMargSmemBins && ctx->totalQbt >= kMargLogTile;
+}
+
 static bool marginal_device(Context* ctx, const int* regs, int nr, double** dOut, long long* outSize) {
   MargDesc D{};
   D.nSel = nr;
@@ -388,9 +523,16 @@ static bool measure(Context* c, const int* regIdxs, int numRegs, double* probsOu
     }
   if (!ready(c, w)) return false;
   arena_reset(c);
+  long long bins = 1;
+  for (int s = 0; s < numRegs; ++s) bins <<= c->q[regIdxs[s]];
   double* dOut;
-  long long outSize;
-  if (!marginal_device(c, regIdxs, numRegs, &dOut, &outSize)) return false;
+  long long outSize = bins;
+  if (tiled_ok(c, bins)) {
+    dOut = (double*)arena_alloc(c, (size_t)bins * sizeof(double));
+    if (!dOut || !marginals_tiled(c, {std::vector<int>(regIdxs, regIdxs + numRegs)}, dOut)) return false;
+  } else if (!marginal_device(c, regIdxs, numRegs, &dOut, &outSize)) {
+    return false;
+  }
   if (!cuda_ok(c, cudaMemcpyAsync(probsOut, dOut, (size_t)outSize * sizeof(double),
                                   cudaMemcpyDeviceToHost, c->stream), "marginal copy"))
     return false;
@@ -410,11 +552,51 @@ void cvdvMeasureMultipleCT(CVDVContext* ctx, const int* regIdxs, int numRegs, do
 void cvdvMeasureEach(CVDVContext* ctx, const int* regIdxs, int numRegs, double* probsOut) {
   if (!ctx) return;
   Context* c = C(ctx);
-  size_t off = 0;
-  for (int k = 0; k < numRegs; ++k) {
-    if (!measure(c, regIdxs + k, 1, probsOut + off, "cvdvMeasureEach")) return;
-    off += (size_t)1 << c->q[regIdxs[k]];
+  const char* w = "cvdvMeasureEach";
+  if (!regIdxs || numRegs <= 0 || numRegs > kMargMaxOut || !probsOut) {
+    set_error(c, kErrInvalidArg, "%s: need 1..%d registers and an output", w, kMargMaxOut);
+    return;
   }
+  for (int k = 0; k < numRegs; ++k)
+    if (regIdxs[k] < 0 || regIdxs[k] >= c->numReg) {
+      set_error(c, kErrInvalidArg, "%s: invalid register index %d", w, regIdxs[k]);
+      return;
+    }
+  // registers whose marginals fit the shared histogram go in one pass; larger
+  // ones are read one at a time
+  std::vector<std::vector<int>> outs;
+  std::vector<size_t> outPos, bigPos;
+  std::vector<int> big;
+  size_t off = 0;
+  long long tiledBins = 0;
+  for (int k = 0; k < numRegs; ++k) {
+    const long long b = 1ll << c->q[regIdxs[k]];
+    if (tiled_ok(c, tiledBins + b)) {
+      outs.push_back({regIdxs[k]});
+      outPos.push_back(off);
+      tiledBins += b;
+    } else {
+      big.push_back(regIdxs[k]);
+      bigPos.push_back(off);
+    }
+    off += (size_t)b;
+  }
+  for (size_t k = 0; k < big.size(); ++k)
+    if (!measure(c, &big[k], 1, probsOut + bigPos[k], w)) return;
+  if (outs.empty()) return;
+  if (!ready(c, w)) return;
+  arena_reset(c);
+  double* dOut = (double*)arena_alloc(c, (size_t)tiledBins * sizeof(double));
+  if (!dOut || !marginals_tiled(c, outs, dOut)) return;
+  size_t src = 0;
+  for (size_t k = 0; k < outs.size(); ++k) {
+    const size_t b = (size_t)1 << c->q[outs[k][0]];
+    if (!cuda_ok(c, cudaMemcpyAsync(probsOut + outPos[k], dOut + src, b * sizeof(double),
+                                    cudaMemcpyDeviceToHost, c->stream), "marginal copy"))
+      return;
+    src += b;
+  }
+  cuda_ok(c, cudaStreamSynchronize(c->stream), "marginal sync");
 }
 
 void cvdvGetFidelity(CVDVContext* ctx, void** devicePtrs, int numReg, double* fidOut) {

@@ -78,7 +78,7 @@ SIGNATURES = [
     ("cvdvGetKernelStats", [c_void_p, POINTER(c_double), POINTER(ctypes.c_longlong), c_int], c_int),
 ]
 
-KERNEL_KINDS = ["fft_pass", "pair", "diag", "perm", "table", "init", "reduce", "phase_space"]
+KERNEL_KINDS = ["fft_pass", "pair", "diag", "perm", "table", "init", "reduce", "phase_space", "seq"]
 
 
 def kernel_stats(ctx):

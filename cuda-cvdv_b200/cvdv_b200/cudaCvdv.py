@@ -52,10 +52,13 @@ class CudaCvdv:
             raise CvdvError(msg)
         self.setFusion(fusion)
 
-    def setFusion(self, on: bool) -> None:
-        """(addition) cancel FtP2Q/FtQ2P pairs separated only by gates on other
-        registers (exact identity; on by default)."""
-        self._L.cvdvSetFusion(self.ctx, 1 if on else 0)
+    def setFusion(self, on) -> None:
+        """(addition) queue optimisations, all on by default: bit 0 cancels
+        FtP2Q/FtQ2P pairs separated only by gates on other registers (exact
+        identity); bit 1 runs chains of qubit gates on up to four qubits as one
+        pass.  True = both, False = neither, an int = those bits."""
+        flags = (3 if on else 0) if isinstance(on, bool) else int(on)
+        self._L.cvdvSetFusion(self.ctx, flags)
 
     def __del__(self):
         try:

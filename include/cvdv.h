@@ -157,8 +157,10 @@ void* cvdvGetStream(CVDVContext* ctx);
 /* Queue optimisations.  flags bit 0 (default on): an FtP2Q(r) followed by an
  * FtQ2P(r) (or the reverse) with only stages that leave register r untouched in
  * between is removed from the queue -- the pair is the identity, so the result
- * is unchanged up to rounding.  cvdvCancelledTransforms counts the transforms
- * removed so far. */
+ * is unchanged up to rounding.  flags bit 1 (default on): consecutive 2x2 qubit
+ * gates on up to four distinct qubits, with the diagonal runs between them, run
+ * as one pass over the state instead of one pass per gate.  cvdvCancelledTransforms
+ * counts the transforms removed so far. */
 void cvdvSetFusion(CVDVContext* ctx, int flags);
 long long cvdvCancelledTransforms(CVDVContext* ctx);
 /* Number of kernels this library has launched in the process so far. */
@@ -167,7 +169,8 @@ unsigned long long cvdvLaunchCount(void);
  * event pair.  cvdvGetKernelStats waits for the stream, returns the number of
  * kernel kinds, fills total milliseconds and launch counts per kind
  * (0 FFT pass, 1 qubit pair, 2 diagonal run, 3 permutation, 4 factor table,
- * 5 initialiser, 6 reduction, 7 phase space) and resets them. */
+ * 5 initialiser, 6 reduction, 7 phase space, 8 qubit-gate sequence) and resets
+ * them. */
 void cvdvSetTiming(CVDVContext* ctx, int on);
 int cvdvGetKernelStats(CVDVContext* ctx, double* msOut, long long* countOut, int n);
 /* Marginals of several single registers in one pass over the state:

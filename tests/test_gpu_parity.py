@@ -230,6 +230,91 @@ def test_transform_cancellation_matches_unfused():
     assert rel(out[True][0], o.get_state()) < PLAIN_TOL
 
 
+def _random_qubit_circuit(rng, qubits, n_gates):
+    """Qubit gates on every qubit of every register but the last (a mode), with
+    conditional displacements and mode gates in between."""
+    mode = len(qubits) - 1
+    sites = [(r, k) for r in range(mode) for k in range(qubits[r])]
+    seq = []
+    for _ in range(n_gates):
+        r, k = sites[rng.integers(len(sites))]
+        g = rng.integers(10)
+        if g == 0:
+            seq.append(("h", (r, k)))
+        elif g == 1:
+            seq.append(("rx", (r, k, float(rng.uniform(0, 2 * np.pi)))))
+        elif g == 2:
+            seq.append(("ry", (r, k, float(rng.uniform(0, 2 * np.pi)))))
+        elif g == 3:
+            seq.append(("rz", (r, k, float(rng.uniform(0, 2 * np.pi)))))
+        elif g == 4:
+            seq.append((("x", "y", "z")[rng.integers(3)], (r, k)))
+        elif g == 5:
+            seq.append(("sheer", (mode, float(rng.uniform(-0.3, 0.3)))))
+        elif g == 6:
+            seq.append(("d", (mode, complex(rng.normal(0, 0.5), rng.normal(0, 0.5)))))
+        else:
+            seq.append(("cd", (mode, r, k, complex(rng.normal(0, 0.5), 0.0))))
+    return seq
+
+
+@pytest.mark.parametrize("qubits", [[1, 1, 1, 1, 1, 1, 8], [3, 2, 7], [1, 2, 1, 3, 1, 6], [2, 2, 2, 9]])
+def test_qubit_gate_sequences(qubits):
+    """Chains of qubit gates run as qubit-gate sequence passes: equal to the oracle
+    (plain and mixed) and to the per-gate pair path."""
+    from cvdv_b200 import _lib
+    rng = np.random.default_rng(sum(qubits) * 7 + len(qubits))
+    n = sum(qubits)
+    psi = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    psi /= np.linalg.norm(psi)
+    seq = _random_qubit_circuit(rng, qubits, 60)
+    o = oracle(qubits, psi)
+    run(o, seq)
+    ref = o.get_state()
+    states = {}
+    for prec, tol, flags in (("complex128", PLAIN_TOL, 3), ("complex128", PLAIN_TOL, 1),
+                             ("complex64", MIXED_TOL, 3)):
+        sim = make(qubits, psi, prec)
+        sim.setFusion(flags)
+        _lib.load().cvdvSetTiming(sim.ctx, 1)
+        run(sim, seq)
+        out = sim.getState()
+        stats = _lib.kernel_stats(sim.ctx)
+        assert rel(out, ref) < tol, (prec, flags)
+        assert (stats["seq"][1] > 0) == (flags == 3), (prec, flags, stats["seq"])
+        states[(prec, flags)] = out
+        if prec == "complex128" and flags == 3:
+            # single-pass marginals of every register, and a joint one
+            each = sim.mEach(list(range(len(qubits))))
+            for r, pr in enumerate(each):
+                np.testing.assert_allclose(pr, o.m(r), atol=1e-13, err_msg=f"mEach {r}")
+            np.testing.assert_allclose(sim.m(len(qubits) - 2, 0), o.m(len(qubits) - 2, 0), atol=1e-13)
+    assert rel(states[("complex128", 3)], states[("complex128", 1)]) < 1e-12
+
+
+def test_state_transfer_uses_sequences():
+    """The headline chain H . CPhaseX . Rz over 14 qubits runs as a few sequence
+    passes (at most four qubits each) between the two mode transforms instead of
+    one pass per qubit."""
+    from cvdv_b200 import CudaCvdv, _lib
+    from cvdv_b200 import workloads as W
+    circ = W.state_transfer(n_qubits=14, mode_qubits=8)
+    sim = CudaCvdv(circ["qubits"], check_errors=True)
+    sim.initStateVector(W.separable_arrays(circ, device="cuda"))
+    W.apply(sim, circ["prep"])
+    sim.synchronize()
+    _lib.load().cvdvSetTiming(sim.ctx, 1)
+    _lib.kernel_stats(sim.ctx)
+    W.apply(sim, circ["gates"])
+    sim.synchronize()
+    st = _lib.kernel_stats(sim.ctx)
+    assert st["seq"][1] >= 3 and st["seq"][1] + st["pair"][1] <= 5, st
+    o = OracleSim(circ["qubits"])
+    o.initStateVector(W.separable_arrays(circ))
+    W.apply(o, circ["prep"] + circ["gates"])
+    assert rel(sim.getState(), o.get_state()) < PLAIN_TOL
+
+
 def test_gaussian_network_scaled():
     from cvdv_b200 import CudaCvdv
     from cvdv_b200 import workloads as W
