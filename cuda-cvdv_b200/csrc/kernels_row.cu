@@ -726,6 +726,207 @@ static cudaError_t launch_rowr(Context* ctx, const RowProgram& P, int q) {
   }
 }
 
+// ---------------------------------------------------------------- two-CTA register-resident rows
+// A row of N = 2 M points (2^14 complex128) is split over a cluster of two CTAs
+// of M/16 threads; every thread keeps 16 amplitudes in registers.  With
+// m_i = t + TPR (8 r + i), i < 8, for thread t of CTA r, two layouts occur:
+//   S ("split natural"): v[i] = x[m_i], v[8 + i] = x[M + m_i];
+//   T ("transposed"):    v[w] = X[r + 2 k2] at k2 = t + TPR w (all 16 w).
+// Forward DFT, S -> T:  y_k1[m] = w_N^{m k1} (x[m] + (-1)^k1 x[M + m]); each CTA
+//   forms both y_0 and y_1 on its own m_i, keeps y_r and hands y_(1-r) to the
+//   sibling through distributed shared memory (8 values per thread); then an
+//   M-point DFT of y_r gives X[r + 2 k2].
+// Inverse DFT, T -> S:  an M-point inverse DFT gives z_r[m] (all 16 w); each CTA
+//   hands the sibling the half of z_r it needs and forms
+//   x[m_i] = z_0 + w_N^{-m} z_1, x[M + m_i] = z_0 - w_N^{-m} z_1.
+// Loads and stores in S are plain coalesced accesses; a program that starts
+// (ends) in T loads (stores) adjacent pairs X[2 k2], X[2 k2 + 1] for the CTA's
+// half of k2 and swaps one of each pair with the sibling.  Diagonal runs in T
+// read tables stored permuted (position r M + k2 holds index r + 2 k2).
+
+// Hand the sibling 8 registers and take 8 of its: this CTA writes its registers
+// SEND_HI (w = 8 SEND_HI + i) at their canonical positions, the sibling does the
+// same, and each reads the other's.  Both CTAs call it with mirrored halves.
+template <typename C, int TPR>
+__device__ __forceinline__ void rc_swap(C* sm, const C* peer, int t, const C (&send)[8], C (&recv)[8],
+                                       int sendHalf, int recvHalf) {
+  cg::cluster_group cl = cg::this_cluster();
+#pragma unroll
+  for (int i = 0; i < 8; ++i) sm[rpad<C>(t + TPR * (8 * sendHalf + i))] = send[i];
+  cl.sync();
+#pragma unroll
+  for (int i = 0; i < 8; ++i) recv[i] = peer[rpad<C>(t + TPR * (8 * recvHalf + i))];
+  cl.sync();  // the sibling has read this CTA's buffer before it is reused
+}
+
+template <typename C, int LOGM>
+__device__ __forceinline__ void rc_diag(C (&v)[16], const RowDiag& D, uint64_t rowBase, int t, int r,
+                                        bool layoutT) {
+  constexpr int TPR = 1 << (LOGM - 4), M = 1 << LOGM;
+  const double2 rs = D.hasRowF ? eval_factor(D.rowF, rowBase) : make_double2(1.0, 0.0);
+  if (D.tab) {
+    int seg = 0;
+    for (int c = 0; c < D.nCtrl; ++c) seg |= (int)((rowBase >> D.ctrlShift[c]) & 1ull) << c;
+    const double2* tp = D.tab + ((size_t)seg << (LOGM + 1));
+    // T: permuted table, index r M + k2; S: natural, index (w >> 3) M + m_(w & 7)
+    const double2* base = layoutT ? tp + r * M + t : tp + t + TPR * 8 * r;
+#pragma unroll
+    for (int k0 = 0; k0 < 16; k0 += 8) {
+      double2 w[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int kk = k0 + k;
+        w[k] = __ldg(base + (layoutT ? TPR * kk : (kk >> 3) * M + TPR * (kk & 7)));
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        if (D.hasRowF) w[k] = dmul(w[k], rs);
+        v[k0 + k] = cmul(v[k0 + k], fromd<C>(w[k]));
+      }
+    }
+  } else if (D.hasRowF) {
+    const C c = fromd<C>(rs);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) v[k] = cmul(v[k], c);
+  }
+}
+
+template <typename C, int LOGN>
+__global__ void __launch_bounds__(1 << (LOGN - 5), 1)
+    k_rowc(const C* __restrict__ in, C* __restrict__ out, const __grid_constant__ RowProgram P) {
+  constexpr int LOGM = LOGN - 1, M = 1 << LOGM, TPR = M >> 4, RS = M + (M >> 4);
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* sm = reinterpret_cast<C*>(smraw);
+  double2* loM = reinterpret_cast<double2*>(sm + RS);  // w_M^e, e < 64
+  double2* hiM = loM + 64;                              // w_M^(64 h), h < M / 64
+  double2* loN = hiM + (M >> 6);                        // w_N^e, e < 64
+  double2* hiN = loN + 64;                              // w_N^(64 h), h < M / 64
+  cg::cluster_group cl = cg::this_cluster();
+  const int r = (int)cl.block_rank();
+  const int t = threadIdx.x;
+  const C* peer = cl.map_shared_rank(sm, r ^ 1);
+  const uint64_t rowBase = ((uint64_t)blockIdx.x >> 1) << LOGN;
+
+  {
+    const int scM = P.logTwN - LOGM, scN = P.logTwN - LOGN;
+    constexpr int NTAB = 2 * (64 + (M >> 6));
+    for (int i = t; i < NTAB; i += TPR) {
+      const int half = i >= NTAB / 2, j = half ? i - NTAB / 2 : i;
+      const int e = j < 64 ? j : (j - 64) << 6;
+      loM[i] = __ldg(P.tw + ((size_t)e << (half ? scN : scM)));  // loM..hiN are one array
+    }
+  }
+  C v[16];
+  bool layoutT = P.loadT != 0;
+  if (!layoutT) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      v[i] = in[rowBase + t + TPR * (8 * r + i)];
+      v[8 + i] = in[rowBase + M + t + TPR * (8 * r + i)];
+    }
+  } else {
+    // pairs X[2 k2], X[2 k2 + 1] for k2 in this CTA's half; keep X[r + 2 k2]
+    C keep[8], give[8], got[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const uint64_t k2 = (uint64_t)(t + TPR * (8 * r + i));
+      const C a = in[rowBase + 2 * k2], b = in[rowBase + 2 * k2 + 1];
+      keep[i] = r ? b : a;
+      give[i] = r ? a : b;
+    }
+    rc_swap<C, TPR>(sm, peer, t, give, got, r, r ^ 1);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      v[r ? 8 + i : i] = keep[i];
+      v[r ? i : 8 + i] = got[i];
+    }
+  }
+  __syncthreads();  // twiddle tables
+
+  for (int o = 0; o < P.nOps; ++o) {
+    const RowOp& op = P.ops[o];
+    if (op.kind == kRowDiag) {
+      rc_diag<C, LOGM>(v, P.diag[op.diag], rowBase, t, r, layoutT);
+    } else if (op.dir > 0) {  // S -> T
+      C mine[8], give[8], got[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int m = t + TPR * (8 * r + i);
+        const C a = v[i], b = v[8 + i];
+        const C y0 = cadd(a, b);
+        const C y1 = cmul(csub(a, b), tw2<C, 1>(loN, hiN, m));
+        mine[i] = r ? y1 : y0;
+        give[i] = r ? y0 : y1;
+      }
+      rc_swap<C, TPR>(sm, peer, t, give, got, r, r ^ 1);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        v[r ? 8 + i : i] = mine[i];
+        v[r ? i : 8 + i] = got[i];
+      }
+      rr_stages<C, 1, LOGM, 0>(v, sm, t, loM, hiM);
+      layoutT = true;
+    } else {  // T -> S
+      rr_stages<C, -1, LOGM, 0>(v, sm, t, loM, hiM);
+      C give[8], got[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) give[i] = v[r ? i : 8 + i];  // the sibling's half of z_r
+      rc_swap<C, TPR>(sm, peer, t, give, got, r ^ 1, r);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int m = t + TPR * (8 * r + i);
+        const C z0 = r ? got[i] : v[i];
+        const C z1 = cmul(r ? v[8 + i] : got[i], tw2<C, -1>(loN, hiN, m));
+        v[i] = cadd(z0, z1);
+        v[8 + i] = csub(z0, z1);
+      }
+      layoutT = false;
+    }
+  }
+
+  if (!layoutT) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      out[rowBase + t + TPR * (8 * r + i)] = v[i];
+      out[rowBase + M + t + TPR * (8 * r + i)] = v[8 + i];
+    }
+  } else {
+    C give[8], got[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) give[i] = v[r ? i : 8 + i];  // X[r + 2 k2] for the sibling's k2
+    rc_swap<C, TPR>(sm, peer, t, give, got, r ^ 1, r);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const uint64_t k2 = (uint64_t)(t + TPR * (8 * r + i));
+      const C own = v[r ? 8 + i : i];
+      out[rowBase + 2 * k2] = r ? got[i] : own;
+      out[rowBase + 2 * k2 + 1] = r ? own : got[i];
+    }
+  }
+}
+
+template <typename C, int LOGN>
+static cudaError_t launch_rowc_t(Context* ctx, const RowProgram& P) {
+  constexpr int M = 1 << (LOGN - 1);
+  const size_t smem = (size_t)(M + (M >> 4)) * sizeof(C) + 2 * (64 + (M >> 6)) * sizeof(double2);
+  auto kern = k_rowc<C, LOGN>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)(ctx->size() >> (LOGN - 1)));
+  cfg.blockDim = dim3(M >> 4);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, (const C*)ctx->state(), (C*)ctx->other(), P);
+}
+
 // ---------------------------------------------------------------- host side
 int row_log_tile(int precision) { return precision == kC128 ? 12 : 13; }
 
@@ -898,6 +1099,25 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
   }
   bool elemF = false;
   for (int d = 0; d < P.nDiag; ++d) elemF |= P.diag[d].hasElemF != 0;
+  // the two-CTA kernel needs transforms that alternate in direction (each forward
+  // leaves the transposed layout an inverse consumes)
+  bool alternating = true;
+  int lastDir = 0;
+  for (int o = 0; o < P.nOps; ++o)
+    if (P.ops[o].kind == kRowFft) {
+      alternating &= P.ops[o].dir != lastDir;
+      lastDir = P.ops[o].dir;
+    }
+  if (ctx->precision == kC128 && q == 14 && logC == 1 && !elemF && alternating) {
+    cudaError_t er;
+    {
+      LaunchScope _ls(ctx, kKFft);
+      er = launch_rowc_t<double2, 14>(ctx, P);
+    }
+    if (!cuda_ok(ctx, er, "row program launch")) return false;
+    ctx->cur ^= 1;
+    return true;
+  }
   if (logC == 0 && !elemF && q <= rowr_max_log(ctx->precision)) {
     cudaError_t er;
     {

@@ -179,6 +179,21 @@ def test_fft_layouts(qubits, reg):
         sim.ftP2Q(reg)
         o.ft_p2q(reg)
         assert rel(sim.getState(), o.get_state()) < tol
+        # two transforms of the same direction in one program, then an inverse-first one
+        sim.ftQ2P(reg)
+        sim.ftQ2P(reg)
+        o.ft_q2p(reg)
+        o.ft_q2p(reg)
+        assert rel(sim.getState(), o.get_state()) < tol
+        sim.sheer(reg, 0.1)
+        sim.ftP2Q(reg)
+        sim.sheer(reg, -0.2)
+        sim.ftQ2P(reg)
+        o.phase_x2(reg, 0.1)
+        o.ft_p2q(reg)
+        o.phase_x2(reg, -0.2)
+        o.ft_q2p(reg)
+        assert rel(sim.getState(), o.get_state()) < tol
 
 
 @pytest.mark.parametrize("n_qubits,mode_qubits", [(3, 10), (4, 13), (2, 14)])
