@@ -369,7 +369,7 @@ static size_t seq_extent(Context* ctx, const std::vector<Op>& ops, size_t i) {
     std::vector<int> nb = bits;
     if (std::find(nb.begin(), nb.end(), op.st->bit) == nb.end()) nb.push_back(op.st->bit);
     const int addDiag = (op.pre.empty() ? 0 : 1) + (op.post.empty() ? 0 : 1);
-    if ((int)nb.size() > kSeqMaxBits || nOps + 1 + addDiag > kSeqMaxOps ||
+    if ((int)nb.size() > seq_max_bits(ctx) || nOps + 1 + addDiag > kSeqMaxOps ||
         nDiag + addDiag > kSeqMaxDiags)
       break;
     bool ok = true;
@@ -384,6 +384,46 @@ static size_t seq_extent(Context* ctx, const std::vector<Op>& ops, size_t i) {
   return j - i;
 }
 
+// Whether a diagonal run depends on flat-index bit b.
+static bool terms_touch_bit(Context* ctx, const std::vector<Term>& terms, int b) {
+  auto inReg = [&](int r) { return r >= 0 && b >= ctx->flw[r] && b < ctx->flw[r] + ctx->q[r]; };
+  for (const Term& t : terms) {
+    if (t.kind == kTermScalar) continue;
+    const bool ctrl = (t.kind == kTermPoly || t.kind == kTermXX) && t.ctrlBit == b;
+    if (inReg(t.r) || ctrl || (t.kind == kTermXX && inReg(t.s))) return true;
+  }
+  return false;
+}
+
+// A qubit gate that opens a chain of qubit gates but is separated from it by a
+// basis change of another register (H(q0) . FtQ2P(mode) . CPhaseX(ctrl q0) ...)
+// commutes with that basis change: move it past the transform and every other
+// commuting stage, so it runs in the chain's qubit-gate sequence instead of in
+// a pass of its own.  Only stages that commute exactly are crossed.
+static void hoist_pairs_past_transforms(Context* ctx, std::vector<Stage>& st) {
+  for (size_t i = 0; i < st.size(); ++i) {
+    if (st[i].kind != kStPair || (i > 0 && st[i - 1].kind == kStPair)) continue;
+    const int b = st[i].bit;
+    size_t j = i + 1;
+    bool crossedFft = false;
+    for (; j < st.size(); ++j) {
+      const Stage& t = st[j];
+      if (t.kind == kStFft) {
+        if (b >= ctx->flw[t.reg] && b < ctx->flw[t.reg] + ctx->q[t.reg]) break;
+        crossedFft = true;
+      } else if (t.kind == kStDiag) {
+        if (terms_touch_bit(ctx, t.terms, b)) break;
+      } else {
+        break;
+      }
+    }
+    if (!crossedFft || j >= st.size() || (st[j].kind != kStDiag && st[j].kind != kStPair)) continue;
+    Stage moved = std::move(st[i]);
+    for (size_t k = i; k + 1 < j; ++k) st[k] = std::move(st[k + 1]);
+    st[j - 1] = std::move(moved);
+  }
+}
+
 bool flush(Context* ctx) {
   if (ctx->pending.empty()) return true;
   if (!ctx->initialized) {
@@ -394,6 +434,7 @@ bool flush(Context* ctx) {
   arena_reset(ctx);
   std::vector<Stage> stages;
   stages.swap(ctx->pending);
+  if (ctx->fuseSeq) hoist_pairs_past_transforms(ctx, stages);
   std::vector<Op> ops;
   std::vector<Term> diag;
   size_t i = 0;

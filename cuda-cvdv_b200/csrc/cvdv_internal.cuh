@@ -326,7 +326,7 @@ bool row_diag_fits(Context* ctx, int reg, const std::vector<Term>& terms);
 bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops);
 // qubit-gate sequences (kernels_seq.cu): 2x2 gates on up to four bits and the
 // diagonal runs between them in one pass
-constexpr int kSeqMaxBits = 4;
+constexpr int kSeqMaxBits = 5;  // complex64; complex128 sequences take at most 4 (seq_max_bits)
 constexpr int kSeqMaxOps = 24;
 constexpr int kSeqMaxDiags = 10;
 constexpr int kSeqMaxTabs = 4;
@@ -339,6 +339,7 @@ struct HostSeqOp {
 // whether a diagonal run can ride in a sequence over `bits` (global bit positions)
 bool seq_diag_ok(Context* ctx, const std::vector<int>& bits, const std::vector<Term>& terms);
 bool launch_seq(Context* ctx, const std::vector<HostSeqOp>& ops);
+int seq_max_bits(Context* ctx);
 // outer[h] = prod over registers but the last of phi_r[j_r(h)], h < 2^(n - q_last)
 bool launch_outer(Context* ctx, const double2* const* regArrays, double2* outer);
 // FFT of the live state along `reg` into `out` (state untouched); `tmp` is the

@@ -25,17 +25,20 @@ namespace cvdv {
 struct SeqTab {
   const double2* ptr;
   int shift, mask, ctrlShift, half;
-  int gbit;  // selected-bit number (0..NB-1) the index depends on, or -1
-  int d1;    // index offset when that bit is set
+  int dep;  // index depends on the run's selected bit
+  int d1;   // index offset when that bit is set
 };
 
 struct SeqDiag {
   double2 scalar;
   int nTab;
+  int g;  // selected-bit number (0..NB-1) the run depends on, or -1
   SeqTab tab[kSeqMaxTabs];
 };
 
-enum SeqOpKind : int { kSeqPair = 0, kSeqPairReal = 1, kSeqDiag = 2 };
+// kSeqPairH: c [[1, 1], [1, -1]] (Hadamard) -- sums and differences, with the
+// real factor c carried along and folded into the next diagonal run
+enum SeqOpKind : int { kSeqPair = 0, kSeqPairReal = 1, kSeqPairH = 2, kSeqDiag = 3 };
 
 struct SeqOp {
   int kind;
@@ -67,7 +70,7 @@ __device__ __forceinline__ void seq_pair(C* v, const double2* m) {
   }
 }
 
-// real 2x2 matrix (H, Ry): four real-by-complex products per butterfly
+// real 2x2 matrix (Ry): four real-by-complex products per butterfly
 template <typename C, int NB, int B>
 __device__ __forceinline__ void seq_pair_real(C* v, const double2* m) {
   using R = typename SeqReal<C>::t;
@@ -82,124 +85,119 @@ __device__ __forceinline__ void seq_pair_real(C* v, const double2* m) {
 }
 
 template <typename C, int NB, int B>
+__device__ __forceinline__ void seq_pair_h(C* v) {
+#pragma unroll
+  for (int k = 0; k < (1 << NB); ++k) {
+    if (k & (1 << B)) continue;
+    const C x = v[k], y = v[k | (1 << B)];
+    v[k] = cadd(x, y);
+    v[k | (1 << B)] = csub(x, y);
+  }
+}
+
+template <typename C, int NB, int B>
 __device__ __forceinline__ void seq_scale(C* v, double2 f0, double2 f1) {
   const C c0 = fromd<C>(f0), c1 = fromd<C>(f1);
 #pragma unroll
   for (int k = 0; k < (1 << NB); ++k) v[k] = cmul(v[k], (k & (1 << B)) ? c1 : c0);
 }
 
-template <typename C, int NB>
-__device__ __forceinline__ void seq_diag(C* v, const SeqDiag& D, uint64_t base) {
-  double2 a = D.scalar;  // factor common to the whole site
-  double2 p0[NB], p1[NB];
-#pragma unroll
-  for (int b = 0; b < NB; ++b) p0[b] = p1[b] = make_double2(1.0, 0.0);
-  unsigned used = 0;
-  for (int t = 0; t < D.nTab; ++t) {
-    const SeqTab& T = D.tab[t];
-    int idx = (int)((base >> T.shift) & (uint64_t)T.mask);
-    if (T.ctrlShift >= 0) idx += (int)((base >> T.ctrlShift) & 1ull) * T.half;
-    const double2 w0 = __ldg(T.ptr + idx);
-    if (T.gbit < 0) {
-      a = dmul(a, w0);
-      continue;
-    }
-    const double2 w1 = __ldg(T.ptr + idx + T.d1);
-#pragma unroll
-    for (int b = 0; b < NB; ++b) {
-      const bool hit = T.gbit == b;
-      p0[b] = dmul(p0[b], hit ? w0 : make_double2(1.0, 0.0));
-      p1[b] = dmul(p1[b], hit ? w1 : make_double2(1.0, 0.0));
-    }
-    used |= 1u << T.gbit;
+#define SEQ_BIT_SWITCH(b, CALL)                          \
+  switch (b) {                                           \
+    case 0: { constexpr int B_ = 0; CALL; } break;       \
+    case 1: if constexpr (NB > 1) { constexpr int B_ = 1; CALL; } break; \
+    case 2: if constexpr (NB > 2) { constexpr int B_ = 2; CALL; } break; \
+    case 3: if constexpr (NB > 3) { constexpr int B_ = 3; CALL; } break; \
+    default: if constexpr (NB > 4) { constexpr int B_ = 4; CALL; } break; \
   }
-  if (!used) {
-    const C c = fromd<C>(a);
-#pragma unroll
-    for (int k = 0; k < (1 << NB); ++k) v[k] = cmul(v[k], c);
-    return;
-  }
-  bool folded = false;
-#pragma unroll
-  for (int b = 0; b < NB; ++b) {
-    if (!(used & (1u << b))) continue;
-    double2 f0 = p0[b], f1 = p1[b];
-    if (!folded) {
-      f0 = dmul(f0, a);
-      f1 = dmul(f1, a);
-      folded = true;
-    }
-    if (b == 0) seq_scale<C, NB, 0>(v, f0, f1);
-    if constexpr (NB > 1) if (b == 1) seq_scale<C, NB, 1>(v, f0, f1);
-    if constexpr (NB > 2) if (b == 2) seq_scale<C, NB, 2>(v, f0, f1);
-    if constexpr (NB > 3) if (b == 3) seq_scale<C, NB, 3>(v, f0, f1);
-  }
-}
 
-template <typename C, int NB>
-__global__ void __launch_bounds__(256, 2) k_seq(C* __restrict__ st, uint64_t nSites,
-                                            const __grid_constant__ SeqProgram P) {
+template <typename C, int NB, typename IDX>
+__global__ void __launch_bounds__(256, 2) k_seq(C* __restrict__ st, IDX nSites,
+                                               const __grid_constant__ SeqProgram P) {
   constexpr int K = 1 << NB;
-  for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < nSites;
-       s += (uint64_t)gridDim.x * blockDim.x) {
+  using R = typename SeqReal<C>::t;
+  // offsets of a site's amplitudes from its base (the same for every site),
+  // kept in shared memory rather than in 2^NB registers per thread
+  __shared__ IDX soff[K];
+  if (threadIdx.x < K) {
+    IDX o = 0;
+    for (int b = 0; b < NB; ++b)
+      if (threadIdx.x & (1u << b)) o += (IDX)1 << P.bits[b];
+    soff[threadIdx.x] = o;
+  }
+  __syncthreads();
+  for (IDX s = (IDX)blockIdx.x * blockDim.x + threadIdx.x; s < nSites; s += (IDX)gridDim.x * blockDim.x) {
     // site base: s with a zero inserted at every selected bit (ascending order)
-    uint64_t base = s;
+    IDX base = s;
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
-      const uint64_t low = (1ull << P.bits[b]) - 1;
+      const IDX low = ((IDX)1 << P.bits[b]) - 1;
       base = ((base & ~low) << 1) | (base & low);
     }
     C v[K];
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      uint64_t o = base;
-#pragma unroll
-      for (int b = 0; b < NB; ++b)
-        if (k & (1 << b)) o |= 1ull << P.bits[b];
-      v[k] = st[o];
-    }
+    for (int k = 0; k < K; ++k) v[k] = st[base + soff[k]];
+    R sc = (R)1;  // pending real factor of Hadamard-type pairs
     for (int o = 0; o < P.nOps; ++o) {
       const SeqOp& op = P.ops[o];
-      if (op.kind == kSeqDiag) {
-        seq_diag<C, NB>(v, P.diag[op.diag], base);
+      if (op.kind == kSeqPairH) {
+        sc *= (R)op.m[0].x;
+        SEQ_BIT_SWITCH(op.bit, (seq_pair_h<C, NB, B_>(v)))
       } else if (op.kind == kSeqPairReal) {
-        if (op.bit == 0) seq_pair_real<C, NB, 0>(v, op.m);
-        if constexpr (NB > 1) if (op.bit == 1) seq_pair_real<C, NB, 1>(v, op.m);
-        if constexpr (NB > 2) if (op.bit == 2) seq_pair_real<C, NB, 2>(v, op.m);
-        if constexpr (NB > 3) if (op.bit == 3) seq_pair_real<C, NB, 3>(v, op.m);
+        SEQ_BIT_SWITCH(op.bit, (seq_pair_real<C, NB, B_>(v, op.m)))
+      } else if (op.kind == kSeqPair) {
+        SEQ_BIT_SWITCH(op.bit, (seq_pair<C, NB, B_>(v, op.m)))
       } else {
-        if (op.bit == 0) seq_pair<C, NB, 0>(v, op.m);
-        if constexpr (NB > 1) if (op.bit == 1) seq_pair<C, NB, 1>(v, op.m);
-        if constexpr (NB > 2) if (op.bit == 2) seq_pair<C, NB, 2>(v, op.m);
-        if constexpr (NB > 3) if (op.bit == 3) seq_pair<C, NB, 3>(v, op.m);
+        const SeqDiag& D = P.diag[op.diag];
+        double2 w0 = D.scalar, w1 = D.scalar;
+        for (int t = 0; t < D.nTab; ++t) {
+          const SeqTab& T = D.tab[t];
+          int idx = (int)((base >> T.shift) & (IDX)T.mask);
+          if (T.ctrlShift >= 0) idx += (int)((base >> T.ctrlShift) & (IDX)1) * T.half;
+          const double2 a = __ldg(T.ptr + idx);
+          const double2 b = T.dep ? __ldg(T.ptr + idx + T.d1) : a;
+          w0 = dmul(w0, a);
+          w1 = dmul(w1, b);
+        }
+        const double dsc = (double)sc;
+        w0 = make_double2(w0.x * dsc, w0.y * dsc);
+        w1 = make_double2(w1.x * dsc, w1.y * dsc);
+        sc = (R)1;
+        if (D.g < 0) {
+          const C c = fromd<C>(w0);
+#pragma unroll
+          for (int k = 0; k < K; ++k) v[k] = cmul(v[k], c);
+        } else {
+          SEQ_BIT_SWITCH(D.g, (seq_scale<C, NB, B_>(v, w0, w1)))
+        }
       }
     }
+    if (sc != (R)1) {
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      uint64_t o = base;
-#pragma unroll
-      for (int b = 0; b < NB; ++b)
-        if (k & (1 << b)) o |= 1ull << P.bits[b];
-      st[o] = v[k];
+      for (int k = 0; k < K; ++k) v[k] = mk(v[k].x * sc, v[k].y * sc);
     }
+#pragma unroll
+    for (int k = 0; k < K; ++k) st[base + soff[k]] = v[k];
   }
 }
 
 // ---------------------------------------------------------------- host side
 
-// Number of selected bits a table of register r (with external control bit
-// ctrl, or -1) depends on.
-static int seq_deps(Context* ctx, const std::vector<int>& bits, int r, int ctrl) {
-  const int lo = ctx->flw[r], hi = lo + ctx->q[r];
-  int n = 0;
-  for (int b : bits) n += ((b >= lo && b < hi) || b == ctrl) ? 1 : 0;
-  return n;
-}
-
 bool seq_diag_ok(Context* ctx, const std::vector<int>& bits, const std::vector<Term>& terms) {
-  // mirror build_factor_list's grouping: one table per (register, external control)
+  // mirror build_factor_list's grouping: one table per (register, external
+  // control); every table may depend on one selected bit, the same for all
   std::vector<std::pair<int, int>> groups;
   std::vector<int> count;
+  int depBit = -1;
+  auto dep_ok = [&](int r, int ctrl) {
+    const int lo = ctx->flw[r], hi = lo + ctx->q[r];
+    for (int b : bits)
+      if ((b >= lo && b < hi) || b == ctrl) {
+        if (depBit >= 0 && depBit != b) return false;
+        depBit = b;
+      }
+    return true;
+  };
   for (const Term& t : terms) {
     if (t.kind == kTermScalar) continue;
     if (t.kind == kTermXX) return false;
@@ -208,12 +206,11 @@ bool seq_diag_ok(Context* ctx, const std::vector<int>& bits, const std::vector<T
       const int lo = ctx->flw[t.r], hi = lo + ctx->q[t.r];
       if (!(t.ctrlBit >= lo && t.ctrlBit < hi)) ctrl = t.ctrlBit;
     }
-    if (seq_deps(ctx, bits, t.r, ctrl) > 1) return false;
+    if (!dep_ok(t.r, ctrl)) return false;
     // an uncontrolled group may be folded into a controlled one of the same register
     if (ctrl < 0)
       for (const Term& u : terms)
-        if (u.kind == kTermPoly && u.r == t.r && u.ctrlBit >= 0 && seq_deps(ctx, bits, t.r, u.ctrlBit) > 1)
-          return false;
+        if (u.kind == kTermPoly && u.r == t.r && u.ctrlBit >= 0 && !dep_ok(t.r, u.ctrlBit)) return false;
     std::pair<int, int> key{t.r, ctrl};
     size_t g = 0;
     while (g < groups.size() && groups[g] != key) ++g;
@@ -228,14 +225,20 @@ bool seq_diag_ok(Context* ctx, const std::vector<int>& bits, const std::vector<T
   return tables <= kSeqMaxTabs;
 }
 
-template <typename C>
+int seq_max_bits(Context* ctx) { return ctx->precision == kC128 ? 4 : 5; }
+
+template <typename C, typename IDX>
 static void seq_dispatch(Context* ctx, int nb, unsigned blocks, uint64_t nSites, const SeqProgram& P) {
   C* st = (C*)ctx->state();
+  const IDX n = (IDX)nSites;
   switch (nb) {
-    case 1: k_seq<C, 1><<<blocks, 256, 0, ctx->stream>>>(st, nSites, P); break;
-    case 2: k_seq<C, 2><<<blocks, 256, 0, ctx->stream>>>(st, nSites, P); break;
-    case 3: k_seq<C, 3><<<blocks, 256, 0, ctx->stream>>>(st, nSites, P); break;
-    default: k_seq<C, 4><<<blocks, 256, 0, ctx->stream>>>(st, nSites, P); break;
+    case 1: k_seq<C, 1, IDX><<<blocks, 256, 0, ctx->stream>>>(st, n, P); break;
+    case 2: k_seq<C, 2, IDX><<<blocks, 256, 0, ctx->stream>>>(st, n, P); break;
+    case 3: k_seq<C, 3, IDX><<<blocks, 256, 0, ctx->stream>>>(st, n, P); break;
+    case 4: k_seq<C, 4, IDX><<<blocks, 256, 0, ctx->stream>>>(st, n, P); break;
+    default:
+      if constexpr (sizeof(C) == sizeof(float2)) k_seq<C, 5, IDX><<<blocks, 256, 0, ctx->stream>>>(st, n, P);
+      break;
   }
 }
 
@@ -245,7 +248,7 @@ bool launch_seq(Context* ctx, const std::vector<HostSeqOp>& ops) {
     if (op.kind == 0 && std::find(bits.begin(), bits.end(), op.bit) == bits.end()) bits.push_back(op.bit);
   std::sort(bits.begin(), bits.end());
   const int nb = (int)bits.size();
-  if (nb < 1 || nb > kSeqMaxBits || (int)ops.size() > kSeqMaxOps) {
+  if (nb < 1 || nb > seq_max_bits(ctx) || (int)ops.size() > kSeqMaxOps) {
     set_error(ctx, kErrUnsupported, "qubit-gate sequence outside the kernel limits");
     return false;
   }
@@ -261,7 +264,8 @@ bool launch_seq(Context* ctx, const std::vector<HostSeqOp>& ops) {
         o.m[k] = h.m[k];
         real = real && h.m[k].y == 0.0;
       }
-      o.kind = real ? kSeqPairReal : kSeqPair;
+      const bool had = real && h.m[0].x == h.m[1].x && h.m[0].x == h.m[2].x && h.m[0].x == -h.m[3].x;
+      o.kind = had ? kSeqPairH : real ? kSeqPairReal : kSeqPair;
       continue;
     }
     if (nd >= kSeqMaxDiags) {
@@ -278,6 +282,7 @@ bool launch_seq(Context* ctx, const std::vector<HostSeqOp>& ops) {
     SeqDiag& D = P.diag[nd];
     D.scalar = F.hasScalar ? F.scalar : make_double2(1.0, 0.0);
     D.nTab = F.nTab;
+    D.g = -1;
     for (int t = 0; t < F.nTab; ++t) {
       const TabFactor& T = F.tab[t];
       SeqTab& S = D.tab[t];
@@ -286,19 +291,20 @@ bool launch_seq(Context* ctx, const std::vector<HostSeqOp>& ops) {
       S.mask = T.mask;
       S.ctrlShift = T.ctrlShift;
       S.half = T.half;
-      S.gbit = -1;
+      S.dep = 0;
       S.d1 = 0;
       for (int b = 0; b < nb; ++b) {
         const uint64_t i = 1ull << bits[b];
         int d = (int)((i >> T.shift) & (uint64_t)T.mask);
         if (T.ctrlShift >= 0) d += (int)((i >> T.ctrlShift) & 1ull) * T.half;
         if (!d) continue;
-        if (S.gbit >= 0) {
-          set_error(ctx, kErrUnsupported, "table depends on two bits of a qubit-gate sequence");
+        if (S.dep || (D.g >= 0 && D.g != b)) {
+          set_error(ctx, kErrUnsupported, "diagonal run depends on two bits of a qubit-gate sequence");
           return false;
         }
-        S.gbit = b;
+        S.dep = 1;
         S.d1 = d;
+        D.g = b;
       }
     }
     o.kind = kSeqDiag;
@@ -307,10 +313,16 @@ bool launch_seq(Context* ctx, const std::vector<HostSeqOp>& ops) {
   const uint64_t nSites = ctx->size() >> nb;
   uint64_t blocks = (nSites + 255) / 256;
   if (blocks > 148ull * 8) blocks = 148ull * 8;
+  const bool narrow = ctx->totalQbt <= 31;  // every flat index fits 32 bits
   {
     LaunchScope _ls(ctx, kKSeq);
-    if (ctx->precision == kC128) seq_dispatch<double2>(ctx, nb, (unsigned)blocks, nSites, P);
-    else seq_dispatch<float2>(ctx, nb, (unsigned)blocks, nSites, P);
+    if (ctx->precision == kC128) {
+      if (narrow) seq_dispatch<double2, uint32_t>(ctx, nb, (unsigned)blocks, nSites, P);
+      else seq_dispatch<double2, uint64_t>(ctx, nb, (unsigned)blocks, nSites, P);
+    } else {
+      if (narrow) seq_dispatch<float2, uint32_t>(ctx, nb, (unsigned)blocks, nSites, P);
+      else seq_dispatch<float2, uint64_t>(ctx, nb, (unsigned)blocks, nSites, P);
+    }
   }
   return cuda_ok(ctx, cudaGetLastError(), "qubit-gate sequence launch");
 }

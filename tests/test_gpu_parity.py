@@ -307,14 +307,15 @@ def test_qubit_gate_sequences(qubits):
     assert rel(states[("complex128", 3)], states[("complex128", 1)]) < 1e-12
 
 
-def test_state_transfer_uses_sequences():
+@pytest.mark.parametrize("precision,passes", [("complex128", 4), ("complex64", 3)])
+def test_state_transfer_uses_sequences(precision, passes):
     """The headline chain H . CPhaseX . Rz over 14 qubits runs as a few sequence
-    passes (at most four qubits each) between the two mode transforms instead of
-    one pass per qubit."""
+    passes (four qubits each in complex128, five in complex64) between the two
+    mode transforms, with the first H moved past the forward transform."""
     from cvdv_b200 import CudaCvdv, _lib
     from cvdv_b200 import workloads as W
     circ = W.state_transfer(n_qubits=14, mode_qubits=8)
-    sim = CudaCvdv(circ["qubits"], check_errors=True)
+    sim = CudaCvdv(circ["qubits"], precision=precision, check_errors=True)
     sim.initStateVector(W.separable_arrays(circ, device="cuda"))
     W.apply(sim, circ["prep"])
     sim.synchronize()
@@ -323,11 +324,12 @@ def test_state_transfer_uses_sequences():
     W.apply(sim, circ["gates"])
     sim.synchronize()
     st = _lib.kernel_stats(sim.ctx)
-    assert st["seq"][1] >= 3 and st["seq"][1] + st["pair"][1] <= 5, st
+    assert st["seq"][1] == passes and st["pair"][1] == 0 and st["fft_pass"][1] == 2, st
     o = OracleSim(circ["qubits"])
     o.initStateVector(W.separable_arrays(circ))
     W.apply(o, circ["prep"] + circ["gates"])
-    assert rel(sim.getState(), o.get_state()) < PLAIN_TOL
+    tol = PLAIN_TOL if precision == "complex128" else MIXED_TOL
+    assert rel(sim.getState(), o.get_state()) < tol
 
 
 def test_gaussian_network_scaled():
