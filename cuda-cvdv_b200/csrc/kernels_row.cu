@@ -563,20 +563,21 @@ __global__ void __launch_bounds__(1 << LOGT, (LOGC > 0 || LOGT > 8) ? 1 : 2)
 
 // ---------------------------------------------------------------- register-resident rows
 // Rows that fit one CTA (up to 2^13 complex128 / 2^14 complex64 points) run in
-// k_rowr: each thread keeps 16 amplitudes of one row in registers for the whole
-// program -- elements t + TPR v (v = 0..15) of its row, TPR = M / 16 threads per
-// row.  A Stockham stage of radix R gives thread t the butterflies j = t + b TPR
-// (b < 16/R); their inputs j + u M/R are exactly the thread's 16 elements
-// (register b + (16/R) u), and the last stage's outputs land on the same
+// k_rowr: each thread keeps E = 16 (or 32) amplitudes of one row in registers
+// for the whole program -- elements t + TPR v (v < E) of its row, TPR = M / E
+// threads per row.  A Stockham stage of radix R gives thread t the butterflies
+// j = t + b TPR (b < E/R); their inputs j + u M/R are exactly the thread's E
+// elements (register b + (E/R) u), and the last stage's outputs land on the same
 // positions.  So the global load, the store and every diagonal run between
 // transforms work on registers in place; only the stages inside a transform
 // exchange data, through one padded shared-memory row.  Row length, radices and
 // strides are template constants, so every shared-memory address is a
 // per-thread base plus an immediate offset.
 
-template <typename C, int DIR, int LOGM, int LOGRAD, int LOGNS>
-__device__ __forceinline__ void rr_butterflies(C (&v)[16], int t, const double2* lo, const double2* hi) {
-  constexpr int RAD = 1 << LOGRAD, NB = 16 / RAD, TPR = 1 << (LOGM - 4);
+template <typename C, int DIR, int LOGM, int LOGRAD, int LOGNS, int LOGE>
+__device__ __forceinline__ void rr_butterflies(C (&v)[1 << LOGE], int t, const double2* lo,
+                                               const double2* hi) {
+  constexpr int E = 1 << LOGE, RAD = 1 << LOGRAD, NB = E / RAD, TPR = 1 << (LOGM - LOGE);
 #pragma unroll
   for (int b = 0; b < NB; ++b) {
     C x[RAD];
@@ -605,9 +606,9 @@ __device__ __forceinline__ void rr_butterflies(C (&v)[16], int t, const double2*
 }
 
 // outputs of a stage to their autosorted positions, then the next stage's inputs
-template <typename C, int LOGM, int LOGRAD, int LOGNS>
-__device__ __forceinline__ void rr_exchange(C (&v)[16], C* smrow, int t) {
-  constexpr int RAD = 1 << LOGRAD, NB = 16 / RAD, TPR = 1 << (LOGM - 4);
+template <typename C, int LOGM, int LOGRAD, int LOGNS, int LOGE>
+__device__ __forceinline__ void rr_exchange(C (&v)[1 << LOGE], C* smrow, int t) {
+  constexpr int E = 1 << LOGE, RAD = 1 << LOGRAD, NB = E / RAD, TPR = 1 << (LOGM - LOGE);
 #pragma unroll
   for (int b = 0; b < NB; ++b) {
     const int j = t + b * TPR;
@@ -617,32 +618,33 @@ __device__ __forceinline__ void rr_exchange(C (&v)[16], C* smrow, int t) {
   }
   __syncthreads();
 #pragma unroll
-  for (int k = 0; k < 16; ++k) v[k] = smrow[rpad<C>(t + k * TPR)];
+  for (int k = 0; k < E; ++k) v[k] = smrow[rpad<C>(t + k * TPR)];
   __syncthreads();
 }
 
-template <typename C, int DIR, int LOGM, int S>
-__device__ __forceinline__ void rr_stages(C (&v)[16], C* smrow, int t, const double2* lo, const double2* hi) {
+template <typename C, int DIR, int LOGM, int S, int LOGE = 4>
+__device__ __forceinline__ void rr_stages(C (&v)[1 << LOGE], C* smrow, int t, const double2* lo,
+                                          const double2* hi) {
   constexpr int N16 = LOGM / 4, REM = LOGM % 4;
   if constexpr (S < N16) {
-    rr_butterflies<C, DIR, LOGM, 4, 4 * S>(v, t, lo, hi);
-    if constexpr (S + 1 < N16 || REM) rr_exchange<C, LOGM, 4, 4 * S>(v, smrow, t);
-    rr_stages<C, DIR, LOGM, S + 1>(v, smrow, t, lo, hi);
+    rr_butterflies<C, DIR, LOGM, 4, 4 * S, LOGE>(v, t, lo, hi);
+    if constexpr (S + 1 < N16 || REM) rr_exchange<C, LOGM, 4, 4 * S, LOGE>(v, smrow, t);
+    rr_stages<C, DIR, LOGM, S + 1, LOGE>(v, smrow, t, lo, hi);
   } else if constexpr (REM > 0) {
-    rr_butterflies<C, DIR, LOGM, REM, 4 * N16>(v, t, lo, hi);
+    rr_butterflies<C, DIR, LOGM, REM, 4 * N16, LOGE>(v, t, lo, hi);
   }
 }
 
-template <typename C, int LOGM>
-__device__ __forceinline__ void rr_diag(C (&v)[16], const RowDiag& D, uint64_t rowBase, int t) {
-  constexpr int TPR = 1 << (LOGM - 4);
+template <typename C, int LOGM, int LOGE>
+__device__ __forceinline__ void rr_diag(C (&v)[1 << LOGE], const RowDiag& D, uint64_t rowBase, int t) {
+  constexpr int E = 1 << LOGE, TPR = 1 << (LOGM - LOGE);
   const double2 rs = D.hasRowF ? eval_factor(D.rowF, rowBase) : make_double2(1.0, 0.0);
   if (D.tab) {
     int seg = 0;
     for (int c = 0; c < D.nCtrl; ++c) seg |= (int)((rowBase >> D.ctrlShift[c]) & 1ull) << c;
     const double2* tp = D.tab + ((size_t)seg << LOGM) + t;
 #pragma unroll
-    for (int k0 = 0; k0 < 16; k0 += 8) {
+    for (int k0 = 0; k0 < E; k0 += 8) {
       double2 w[8];
 #pragma unroll
       for (int k = 0; k < 8; ++k) w[k] = __ldg(tp + (k0 + k) * TPR);
@@ -655,21 +657,21 @@ __device__ __forceinline__ void rr_diag(C (&v)[16], const RowDiag& D, uint64_t r
   } else if (D.hasRowF) {
     const C c = fromd<C>(rs);
 #pragma unroll
-    for (int k = 0; k < 16; ++k) v[k] = cmul(v[k], c);
+    for (int k = 0; k < E; ++k) v[k] = cmul(v[k], c);
   }
 }
 
 // 256-thread CTAs run two per SM; 512- and 1024-thread CTAs one
-template <typename C, int LOGM, int LOGR>
-__global__ void __launch_bounds__(1 << (LOGM - 4 + LOGR), (LOGM - 4 + LOGR) > 8 ? 1 : 2)
+template <typename C, int LOGM, int LOGR, int LOGE>
+__global__ void __launch_bounds__(1 << (LOGM - LOGE + LOGR), (LOGM - LOGE + LOGR) > 8 ? 1 : 2)
     k_rowr(const C* __restrict__ in, C* __restrict__ out, const __grid_constant__ RowProgram P) {
-  constexpr int M = 1 << LOGM, TPR = M >> 4, NT = TPR << LOGR, RS = M + (M >> 4);
+  constexpr int E = 1 << LOGE, M = 1 << LOGM, TPR = M >> LOGE, NT = TPR << LOGR, RS = M + (M >> 4);
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
   double2* lo = reinterpret_cast<double2*>(sm + (RS << LOGR));  // w_M^e, e < 64
   double2* hi = lo + 64;                                         // w_M^(64 h), h < M / 64
   const int tid = threadIdx.x;
-  const int row = tid >> (LOGM - 4);
+  const int row = tid >> (LOGM - LOGE);
   const int t = tid & (TPR - 1);
   C* smrow = sm + row * RS;
   const uint64_t rowBase = ((uint64_t)blockIdx.x << (LOGM + LOGR)) + ((uint64_t)row << LOGM);
@@ -679,31 +681,39 @@ __global__ void __launch_bounds__(1 << (LOGM - 4 + LOGR), (LOGM - 4 + LOGR) > 8 
     const int e = i < 64 ? i : (i - 64) << 6;
     lo[i] = __ldg(P.tw + ((size_t)e << scM));  // lo and hi are one array
   }
-  C v[16];
+  C v[E];
 #pragma unroll
-  for (int k = 0; k < 16; ++k) v[k] = in[rowBase + t + k * TPR];
+  for (int k = 0; k < E; ++k) v[k] = in[rowBase + t + k * TPR];
   __syncthreads();
 
   for (int o = 0; o < P.nOps; ++o) {
     const RowOp& op = P.ops[o];
-    if (op.kind == kRowDiag) rr_diag<C, LOGM>(v, P.diag[op.diag], rowBase, t);
-    else if (op.dir > 0) rr_stages<C, 1, LOGM, 0>(v, smrow, t, lo, hi);
-    else rr_stages<C, -1, LOGM, 0>(v, smrow, t, lo, hi);
+    if (op.kind == kRowDiag) rr_diag<C, LOGM, LOGE>(v, P.diag[op.diag], rowBase, t);
+    else if (op.dir > 0) rr_stages<C, 1, LOGM, 0, LOGE>(v, smrow, t, lo, hi);
+    else rr_stages<C, -1, LOGM, 0, LOGE>(v, smrow, t, lo, hi);
   }
 #pragma unroll
-  for (int k = 0; k < 16; ++k) out[rowBase + t + k * TPR] = v[k];
+  for (int k = 0; k < E; ++k) out[rowBase + t + k * TPR] = v[k];
 }
 
-// largest row k_rowr takes (one CTA: 16 amplitudes x 512 / 1024 threads)
+// largest row k_rowr takes (one CTA: 2^13 complex128 / 2^14 complex64 points)
 static int rowr_max_log(int precision) { return precision == kC128 ? 13 : 14; }
+
+// complex64 rows of 2^13 and 2^14 points keep 32 amplitudes per thread (256 / 512
+// threads); everything else 16
+template <typename C, int LOGM>
+struct RrShape {
+  static constexpr int LOGE = (sizeof(C) == sizeof(float2) && LOGM >= 13) ? 5 : 4;
+  static constexpr int LOGR = LOGM - LOGE < 8 ? 8 - (LOGM - LOGE) : 0;
+};
 
 template <typename C, int LOGM>
 static cudaError_t launch_rowr_t(Context* ctx, const RowProgram& P) {
-  constexpr int LOGR = LOGM < 12 ? 12 - LOGM : 0;
-  constexpr int NT = 1 << (LOGM - 4 + LOGR);
+  constexpr int LOGE = RrShape<C, LOGM>::LOGE, LOGR = RrShape<C, LOGM>::LOGR;
+  constexpr int NT = 1 << (LOGM - LOGE + LOGR);
   constexpr int M = 1 << LOGM;
   const size_t smem = (size_t)(M + (M >> 4)) * (1 << LOGR) * sizeof(C) + (64 + (M >> 6)) * sizeof(double2);
-  auto kern = k_rowr<C, LOGM, LOGR>;
+  auto kern = k_rowr<C, LOGM, LOGR, LOGE>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const uint64_t nCta = ctx->size() >> (LOGM + LOGR);
@@ -864,10 +874,10 @@ __global__ void __launch_bounds__(1 << (LOGN - 5), 1)
         v[r ? 8 + i : i] = mine[i];
         v[r ? i : 8 + i] = got[i];
       }
-      rr_stages<C, 1, LOGM, 0>(v, sm, t, loM, hiM);
+      rr_stages<C, 1, LOGM, 0, 4>(v, sm, t, loM, hiM);
       layoutT = true;
     } else {  // T -> S
-      rr_stages<C, -1, LOGM, 0>(v, sm, t, loM, hiM);
+      rr_stages<C, -1, LOGM, 0, 4>(v, sm, t, loM, hiM);
       C give[8], got[8];
 #pragma unroll
       for (int i = 0; i < 8; ++i) give[i] = v[r ? i : 8 + i];  // the sibling's half of z_r
