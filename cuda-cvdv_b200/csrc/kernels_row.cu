@@ -38,6 +38,7 @@
 #include <cooperative_groups.h>
 
 #include "cvdv_internal.cuh"
+#include "row_fft.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -84,113 +85,6 @@ struct RowProgram {
   RowDiag diag[kMaxRowDiags];
 };
 
-// shared-memory position of element e of a row: one padding slot every 16
-// (the radix-16 stride), which keeps the strided butterfly accesses conflict-free
-template <typename C>
-__device__ __forceinline__ int rpad(int e) {
-  return e + (e >> 4);
-}
-
-// ---------------------------------------------------------------- butterflies
-template <typename C, int DIR>
-__device__ __forceinline__ C rot_mi(C a) {  // * (-DIR i)
-  return DIR > 0 ? mk(a.y, -a.x) : mk(-a.y, a.x);
-}
-
-template <typename C, int DIR>
-__device__ __forceinline__ void bf2(C& a, C& b) {
-  C t = a;
-  a = cadd(t, b);
-  b = csub(t, b);
-}
-
-template <typename C, int DIR>
-__device__ __forceinline__ void bf4(C& a0, C& a1, C& a2, C& a3) {
-  C s02 = cadd(a0, a2), d02 = csub(a0, a2);
-  C s13 = cadd(a1, a3), d13 = rot_mi<C, DIR>(csub(a1, a3));
-  a0 = cadd(s02, s13);
-  a2 = csub(s02, s13);
-  a1 = cadd(d02, d13);
-  a3 = csub(d02, d13);
-}
-
-// multiply by w8^K, w8 = exp(-DIR i pi / 4)
-template <typename C, int DIR, int K>
-__device__ __forceinline__ C w8mul(C o) {
-  using T = decltype(o.x);
-  const T h = (T)0.70710678118654752440;
-  if constexpr (K == 0) return o;
-  else if constexpr (K == 1)
-    return DIR > 0 ? mk(h * (o.x + o.y), h * (o.y - o.x)) : mk(h * (o.x - o.y), h * (o.y + o.x));
-  else if constexpr (K == 2) return rot_mi<C, DIR>(o);
-  else
-    return DIR > 0 ? mk(h * (o.y - o.x), -h * (o.x + o.y)) : mk(-h * (o.x + o.y), h * (o.x - o.y));
-}
-
-template <typename C, int DIR>
-__device__ __forceinline__ void bf8(C* v) {
-  C e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
-  C o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
-  bf4<C, DIR>(e0, e1, e2, e3);
-  bf4<C, DIR>(o0, o1, o2, o3);
-  o1 = w8mul<C, DIR, 1>(o1);
-  o2 = w8mul<C, DIR, 2>(o2);
-  o3 = w8mul<C, DIR, 3>(o3);
-  v[0] = cadd(e0, o0);
-  v[4] = csub(e0, o0);
-  v[1] = cadd(e1, o1);
-  v[5] = csub(e1, o1);
-  v[2] = cadd(e2, o2);
-  v[6] = csub(e2, o2);
-  v[3] = cadd(e3, o3);
-  v[7] = csub(e3, o3);
-}
-
-// radix 16 = 4 x 4: y[k1 + 4 k2] = sum_n2 w4^{n2 k2} [ w16^{n2 k1} sum_n1 w4^{n1 k1} x[4 n1 + n2] ]
-template <typename C, int DIR>
-__device__ __forceinline__ void bf16(C* v) {
-  using T = decltype(v[0].x);
-  const T c1 = (T)0.92387953251128675613, s1 = (T)0.38268343236508977173;
-  const T sg = DIR > 0 ? (T)-1 : (T)1;  // sign of the imaginary part of w16
-  C a[16];
-#pragma unroll
-  for (int n2 = 0; n2 < 4; ++n2) {
-    C x0 = v[n2], x1 = v[4 + n2], x2 = v[8 + n2], x3 = v[12 + n2];
-    bf4<C, DIR>(x0, x1, x2, x3);
-    a[n2 * 4 + 0] = x0;
-    a[n2 * 4 + 1] = x1;
-    a[n2 * 4 + 2] = x2;
-    a[n2 * 4 + 3] = x3;
-  }
-  auto mulw = [&](C x, T c, T s) { return mk(x.x * c - x.y * s, x.x * s + x.y * c); };
-  a[5] = mulw(a[5], c1, sg * s1);     // w^1
-  a[6] = w8mul<C, DIR, 1>(a[6]);      // w^2
-  a[7] = mulw(a[7], s1, sg * c1);     // w^3
-  a[9] = w8mul<C, DIR, 1>(a[9]);      // w^2
-  a[10] = rot_mi<C, DIR>(a[10]);      // w^4
-  a[11] = w8mul<C, DIR, 3>(a[11]);    // w^6
-  a[13] = mulw(a[13], s1, sg * c1);   // w^3
-  a[14] = w8mul<C, DIR, 3>(a[14]);    // w^6
-  a[15] = mulw(a[15], -c1, -sg * s1); // w^9 = -w^1
-#pragma unroll
-  for (int k1 = 0; k1 < 4; ++k1) {
-    C y0 = a[k1], y1 = a[4 + k1], y2 = a[8 + k1], y3 = a[12 + k1];
-    bf4<C, DIR>(y0, y1, y2, y3);
-    v[k1 + 0] = y0;
-    v[k1 + 4] = y1;
-    v[k1 + 8] = y2;
-    v[k1 + 12] = y3;
-  }
-}
-
-template <typename C, int DIR, int RHO>
-__device__ __forceinline__ void bfly(C* v) {
-  if constexpr (RHO == 16) bf16<C, DIR>(v);
-  else if constexpr (RHO == 8) bf8<C, DIR>(v);
-  else if constexpr (RHO == 4) bf4<C, DIR>(v[0], v[1], v[2], v[3]);
-  else bf2<C, DIR>(v[0], v[1]);
-}
-
 // ---------------------------------------------------------------- twiddles in smem
 // w_L^e = hi[e >> 6] * lo[e & 63] for e < L (L = M for the CTA-local DFT, N for
 // the cross-cluster butterfly); forward convention exp(-2 pi i e / L).
@@ -200,14 +94,6 @@ struct TwTables {
   double2* loN;
   double2* hiN;
 };
-
-template <typename C, int DIR>
-__device__ __forceinline__ C tw2(const double2* lo, const double2* hi, int e) {
-  double2 a = hi[e >> 6], b = lo[e & 63];
-  double2 w = make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-  if (DIR < 0) w.y = -w.y;
-  return fromd<C>(w);
-}
 
 // One Stockham stage of radix RHO, in place on the single tile buffer: every
 // thread gathers its butterflies' operands into registers, the CTA syncs, and
@@ -573,67 +459,6 @@ __global__ void __launch_bounds__(1 << LOGT, (LOGC > 0 || LOGT > 8) ? 1 : 2)
 // exchange data, through one padded shared-memory row.  Row length, radices and
 // strides are template constants, so every shared-memory address is a
 // per-thread base plus an immediate offset.
-
-template <typename C, int DIR, int LOGM, int LOGRAD, int LOGNS, int LOGE>
-__device__ __forceinline__ void rr_butterflies(C (&v)[1 << LOGE], int t, const double2* lo,
-                                               const double2* hi) {
-  constexpr int E = 1 << LOGE, RAD = 1 << LOGRAD, NB = E / RAD, TPR = 1 << (LOGM - LOGE);
-#pragma unroll
-  for (int b = 0; b < NB; ++b) {
-    C x[RAD];
-#pragma unroll
-    for (int u = 0; u < RAD; ++u) x[u] = v[b + NB * u];
-    if constexpr (LOGNS > 0) {
-      const int jm = (t + b * TPR) & ((1 << LOGNS) - 1);
-      // w_{ns R}^{jm u} = w_M^{(jm u) << (LOGM - LOGNS - LOGRAD)}; powers as a tree
-      C w[RAD];
-      w[1] = tw2<C, DIR>(lo, hi, jm << (LOGM - LOGNS - LOGRAD));
-#pragma unroll
-      for (int p = 1; p < RAD / 2; p <<= 1) {
-        w[2 * p] = cmul(w[p], w[p]);
-#pragma unroll
-        for (int u = 1; u < p; ++u) w[p + u] = cmul(w[p], w[u]);
-      }
-#pragma unroll
-      for (int u = RAD / 2 + 1; u < RAD; ++u) w[u] = cmul(w[RAD / 2], w[u - RAD / 2]);
-#pragma unroll
-      for (int u = 1; u < RAD; ++u) x[u] = cmul(x[u], w[u]);
-    }
-    bfly<C, DIR, RAD>(x);
-#pragma unroll
-    for (int u = 0; u < RAD; ++u) v[b + NB * u] = x[u];
-  }
-}
-
-// outputs of a stage to their autosorted positions, then the next stage's inputs
-template <typename C, int LOGM, int LOGRAD, int LOGNS, int LOGE>
-__device__ __forceinline__ void rr_exchange(C (&v)[1 << LOGE], C* smrow, int t) {
-  constexpr int E = 1 << LOGE, RAD = 1 << LOGRAD, NB = E / RAD, TPR = 1 << (LOGM - LOGE);
-#pragma unroll
-  for (int b = 0; b < NB; ++b) {
-    const int j = t + b * TPR;
-    const int y = ((j >> LOGNS) << (LOGNS + LOGRAD)) + (j & ((1 << LOGNS) - 1));
-#pragma unroll
-    for (int u = 0; u < RAD; ++u) smrow[rpad<C>(y + (u << LOGNS))] = v[b + NB * u];
-  }
-  __syncthreads();
-#pragma unroll
-  for (int k = 0; k < E; ++k) v[k] = smrow[rpad<C>(t + k * TPR)];
-  __syncthreads();
-}
-
-template <typename C, int DIR, int LOGM, int S, int LOGE = 4>
-__device__ __forceinline__ void rr_stages(C (&v)[1 << LOGE], C* smrow, int t, const double2* lo,
-                                          const double2* hi) {
-  constexpr int N16 = LOGM / 4, REM = LOGM % 4;
-  if constexpr (S < N16) {
-    rr_butterflies<C, DIR, LOGM, 4, 4 * S, LOGE>(v, t, lo, hi);
-    if constexpr (S + 1 < N16 || REM) rr_exchange<C, LOGM, 4, 4 * S, LOGE>(v, smrow, t);
-    rr_stages<C, DIR, LOGM, S + 1, LOGE>(v, smrow, t, lo, hi);
-  } else if constexpr (REM > 0) {
-    rr_butterflies<C, DIR, LOGM, REM, 4 * N16, LOGE>(v, t, lo, hi);
-  }
-}
 
 template <typename C, int LOGM, int LOGE>
 __device__ __forceinline__ void rr_diag(C (&v)[1 << LOGE], const RowDiag& D, uint64_t rowBase, int t) {

@@ -71,6 +71,12 @@ SIGNATURES = [
     ("cvdvMeasureEach", [c_void_p, POINTER(c_int), c_int, POINTER(c_double)], None),
     ("cvdvMeasureMultipleNoAlloc",
      [c_void_p, c_int, POINTER(c_int), c_int, POINTER(c_int), c_int, c_void_p, c_void_p], c_int),
+    ("cvdvBatchRx", [c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_double, c_void_p], c_int),
+    ("cvdvBatchCondDisp", [c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_double, c_void_p], c_int),
+    ("cvdvBatchRxAdjoint", [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p], c_int),
+    ("cvdvBatchCondDispAdjoint",
+     [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p], c_int),
+    ("cvdvBatchOverlap", [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_void_p], c_int),
     ("cvdvLaunchCount", [], ctypes.c_ulonglong),
     ("cvdvSetFusion", [c_void_p, c_int], None),
     ("cvdvCancelledTransforms", [c_void_p], ctypes.c_longlong),

@@ -19,6 +19,11 @@ All random draws come from ``numpy.random.default_rng(seed)`` in gate order.
   marginals and the Wigner function of mode 0.
 * ``qubit_mode`` -- [1, 10]: qubit |0>, coherent(2+1j); H, cd(1.5), r(0.3),
   s(0.2), H.  Readout: state, both marginals, Wigner of the mode.
+* ``variational`` -- [1, 12], a batch of 64 parameter sets: 40 layers of
+  (Rx(theta_l) on the qubit, cd(beta_l) controlled by it), theta ~ U[0, 2pi),
+  beta ~ N(0, 0.5) real.  Start: qubit |0> x mode vacuum (the configuration names
+  no start state; the vacuum is the choice here).  Target: qubit |0> x the
+  normalised even cat |2> + |-2>.  Loss 1 - |<target|psi>|^2.
 """
 
 from __future__ import annotations
@@ -89,3 +94,33 @@ def apply(sim, gates: List[Gate]) -> None:
     """Run (method, args) pairs on any object with the CudaCvdv gate API."""
     for meth, args in gates:
         getattr(sim, meth)(*args)
+
+
+def variational(seed: int = 5, batch: int = 64, mode_qubits: int = 12, layers: int = 40) -> Dict[str, Any]:
+    rng = np.random.default_rng(seed)
+    theta = rng.uniform(0.0, 2.0 * math.pi, size=(batch, layers))
+    beta = rng.normal(0.0, 0.5, size=(batch, layers))
+    params = np.empty((batch, 2 * layers))
+    params[:, 0::2] = theta
+    params[:, 1::2] = beta
+    qubits = [1, mode_qubits]
+    init = [("setZero", ()), ("setFock", (0,))]
+    target = [("setZero", ()), ("setCat", ([(2.0, 1.0), (-2.0, 1.0)],))]
+    gates: List[Gate] = []
+    for _ in range(layers):
+        gates += [("rx", (0, 0)), ("cd", (1, 0, 0))]
+    return dict(name="variational", qubits=qubits, init=init, target=target, gates=gates, params=params,
+                seed=seed)
+
+
+def product_state(qubits, setters, device: str = "cpu"):
+    """Flat state vector (complex128 torch tensor) of a separable state."""
+    import torch
+    from .separable import SeparableState
+    sep = SeparableState(qubits, device=device)
+    for r, (meth, args) in enumerate(setters):
+        getattr(sep, meth)(r, *args)
+    psi = sep.register_arrays[0]
+    for a in sep.register_arrays[1:]:
+        psi = torch.outer(psi, a).reshape(-1)
+    return psi

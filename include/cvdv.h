@@ -176,6 +176,35 @@ int cvdvGetKernelStats(CVDVContext* ctx, double* msOut, long long* countOut, int
 /* Marginals of several single registers in one pass over the state:
  * probsOut receives, for each k, dims[regIdxs[k]] values back to back. */
 void cvdvMeasureEach(CVDVContext* ctx, const int* regIdxs, int numRegs, double* probsOut);
+/* ---------------------------------------------------------------- batched
+ * variational circuits (no reference counterpart; the reference's TorchCvdv is
+ * not differentiable in its gate parameters).  A batch is one caller-owned
+ * device array of `batch` states of n qubits each (complex128 or complex64 per
+ * precision, instance b at offset b 2^n), laid out [qubit registers..., mode]
+ * with the mode the last register.  Each instance has its own parameter per
+ * gate (device arrays of `batch` doubles).  Every call only enqueues work on
+ * `stream` and returns 0 or an error code (message via cvdvGetLastError(NULL)).
+ *
+ * Rx(sign * thetas[b]) on flat bit `bit` of every instance. */
+int cvdvBatchRx(void* states, int precision, int batch, int n, int bit, const double* thetas, double sign,
+                void* stream);
+/* cd(sign * betas[b]) with a real displacement (src/cuda/gates.cu:163-204) on a
+ * mode of modeQubits (8..12) bits, controlled by flat bit ctrlBit. */
+int cvdvBatchCondDisp(void* states, int precision, int batch, int n, int modeQubits, int ctrlBit,
+                      const double* betas, double sign, void* stream);
+/* Adjoint steps.  With psi the state after the gate and lam the back-propagated
+ * target, write g_b = <lam_b| G |psi_b> (complex, gOut[2b], gOut[2b+1], device)
+ * for the gate's generator G (Rx(theta) = exp(-i theta X/2): G = -X/2; cd(beta)
+ * = exp(i beta G)) and apply the inverse gate to both arrays. */
+int cvdvBatchRxAdjoint(void* psi, void* lam, int precision, int batch, int n, int bit, const double* thetas,
+                       double* gOut, void* stream);
+int cvdvBatchCondDispAdjoint(void* psi, void* lam, int precision, int batch, int n, int modeQubits,
+                             int ctrlBit, const double* betas, double* gOut, void* stream);
+/* out[2b], out[2b+1] = <target| states_b> (target shared by every instance, or
+ * one per instance when targetPerInstance != 0). */
+int cvdvBatchOverlap(const void* states, const void* target, int precision, int batch, int n,
+                     int targetPerInstance, double* out, void* stream);
+
 /* No counterpart in the reference.  The joint marginal of cvdvMeasureMultiple
  * for callers that cannot let the library allocate device memory (their device
  * memory belongs to another allocator, is fixed at start-up, or must not see

@@ -1,0 +1,139 @@
+"""Batched variational circuits: forward parity with the oracle, adjoint
+gradients against central finite differences and against autograd through a
+differentiable complex128 torch restatement of the same gates.
+
+The reference cannot be differentiated (TorchCvdv casts gate parameters to
+Python scalars), so the gradients are pinned by finite differences of the
+oracle-checked forward pass."""
+
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from oracle.cvdv_oracle import OracleSim
+
+pytestmark = pytest.mark.gpu
+
+
+def _circ(precision, layers, mode_qubits, checkpoint_every=16):
+    from cvdv_b200 import workloads as W
+    from cvdv_b200.variational import VariationalCircuit, layered_gates
+    return VariationalCircuit([1, mode_qubits], layered_gates(layers), precision=precision,
+                              checkpoint_every=checkpoint_every)
+
+
+def _problem(batch, layers, mode_qubits, seed=5):
+    from cvdv_b200 import workloads as W
+    w = W.variational(seed=seed, batch=batch, mode_qubits=mode_qubits, layers=layers)
+    psi0 = W.product_state(w["qubits"], w["init"])
+    tgt = W.product_state(w["qubits"], w["target"])
+    return w, torch.tensor(w["params"]), psi0, tgt
+
+
+def _oracle_state(qubits, params_row, psi0):
+    o = OracleSim(qubits)
+    o.set_state(psi0.numpy())
+    for l in range(len(params_row) // 2):
+        o.rx(0, 0, float(params_row[2 * l]))
+        o.cd(1, 0, 0, float(params_row[2 * l + 1]))
+    return o.get_state()
+
+
+@pytest.mark.parametrize("precision,tol", [("complex128", 1e-10), ("complex64", 2e-5)])
+def test_forward_matches_oracle(precision, tol):
+    w, params, psi0, tgt = _problem(batch=6, layers=5, mode_qubits=10)
+    circ = _circ(precision, 5, 10)
+    out = circ.states(params, psi0).cpu().numpy()
+    for b in range(params.shape[0]):
+        ref = _oracle_state(w["qubits"], params[b].numpy(), psi0)
+        assert np.linalg.norm(out[b] - ref) / np.linalg.norm(ref) < tol, b
+    loss = circ.fidelity_loss(params, psi0, tgt).cpu().numpy()
+    ref_loss = [1 - abs(np.vdot(tgt.numpy(), _oracle_state(w["qubits"], params[b].numpy(), psi0))) ** 2
+                for b in range(params.shape[0])]
+    np.testing.assert_allclose(loss, ref_loss, atol=10 * tol)
+
+
+def test_adjoint_matches_central_differences():
+    """complex128 adjoint vs central differences (h = 1e-4) of the complex128 forward."""
+    layers, mq = 8, 10
+    w, params, psi0, tgt = _problem(batch=2, layers=layers, mode_qubits=mq)
+    circ = _circ("complex128", layers, mq, checkpoint_every=4)
+    p = params.clone().requires_grad_(True)
+    circ.fidelity_loss(p, psi0, tgt).sum().backward()
+    grad = p.grad.numpy()
+    h = 1e-4
+    P = params.shape[1]
+    # every perturbed parameter set is one instance of a single batched forward
+    plus = params.repeat_interleave(P, dim=0)
+    minus = plus.clone()
+    idx = torch.arange(P).repeat(params.shape[0])
+    plus[torch.arange(plus.shape[0]), idx] += h
+    minus[torch.arange(minus.shape[0]), idx] -= h
+    with torch.no_grad():
+        lp = circ.fidelity_loss(plus, psi0, tgt).cpu().numpy()
+        lm = circ.fidelity_loss(minus, psi0, tgt).cpu().numpy()
+    fd = ((lp - lm) / (2 * h)).reshape(params.shape[0], P)
+    scale = np.abs(fd).max()
+    assert np.abs(grad - fd).max() < 1e-6 * scale + 1e-9, np.abs(grad - fd).max() / scale
+
+
+def _torch_forward(params, psi0, layers, mq):
+    """Differentiable complex128 restatement: Rx on the qubit, cd = FtP2Q exp(i beta K) FtQ2P."""
+    N = 1 << mq
+    j = torch.arange(N, dtype=torch.float64)
+    dx = math.sqrt(2 * math.pi / N)
+    x = (j - (N - 1) / 2) * dx
+    th = math.pi * (N - 1) * (2 * j - N + 1) / (2 * N)
+    pre = torch.exp(1j * th)
+    glob = complex(np.exp(1j * math.pi * (N - 1) ** 2 / (2 * N)))
+    psi = psi0.reshape(2, N).to(torch.complex128)
+    for l in range(layers):
+        t, b = params[2 * l], params[2 * l + 1]
+        c, s = torch.cos(t / 2), torch.sin(t / 2)
+        psi = torch.stack([c * psi[0] - 1j * s * psi[1], -1j * s * psi[0] + c * psi[1]])
+        z = torch.tensor([1.0, -1.0], dtype=torch.float64)[:, None]
+        P = torch.fft.fft(psi * pre, dim=1) * pre * glob / math.sqrt(N)
+        P = P * torch.exp(1j * (-math.sqrt(2) * b) * z * x)
+        Q = torch.fft.ifft(P * pre.conj() * np.conj(glob), dim=1) * math.sqrt(N) * pre.conj()
+        psi = Q
+    return psi.reshape(-1)
+
+
+def test_adjoint_matches_torch_autograd_and_mixed_precision():
+    layers, mq = 6, 10
+    w, params, psi0, tgt = _problem(batch=3, layers=layers, mode_qubits=mq)
+    # the restatement's forward is pinned to the oracle first
+    ref = _oracle_state(w["qubits"], params[0].numpy(), psi0)
+    np.testing.assert_allclose(_torch_forward(params[0], psi0, layers, mq).numpy(), ref, atol=1e-12)
+    auto = []
+    for b in range(params.shape[0]):
+        p = params[b].clone().requires_grad_(True)
+        psi = _torch_forward(p, psi0, layers, mq)
+        loss = 1 - torch.abs(torch.vdot(tgt.to(torch.complex128), psi)) ** 2
+        loss.backward()
+        auto.append(p.grad.numpy())
+    auto = np.array(auto)
+    for precision, tol in (("complex128", 1e-9), ("complex64", 2e-4)):
+        circ = _circ(precision, layers, mq, checkpoint_every=4)
+        p = params.clone().requires_grad_(True)
+        circ.fidelity_loss(p, psi0, tgt).sum().backward()
+        err = np.abs(p.grad.numpy() - auto).max() / np.abs(auto).max()
+        assert err < tol, (precision, err)
+
+
+def test_full_config_gradient_step():
+    """The configured problem: 64 parameter sets, [1, 12], 40 layers, complex64,
+    checkpoints every 8 layers; gradients agree with the complex128 adjoint."""
+    w, params, psi0, tgt = _problem(batch=64, layers=40, mode_qubits=12)
+    grads = {}
+    for precision in ("complex64", "complex128"):
+        circ = _circ(precision, 40, 12, checkpoint_every=16)
+        p = params.clone().requires_grad_(True)
+        loss = circ.fidelity_loss(p, psi0, tgt)
+        loss.sum().backward()
+        assert torch.isfinite(loss).all() and (loss >= -1e-6).all() and (loss <= 1 + 1e-6).all()
+        grads[precision] = p.grad.numpy()
+    err = np.abs(grads["complex64"] - grads["complex128"]).max() / np.abs(grads["complex128"]).max()
+    assert err < 1e-3, err
