@@ -77,6 +77,8 @@ SIGNATURES = [
     ("cvdvBatchCondDispAdjoint",
      [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p], c_int),
     ("cvdvBatchOverlap", [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_void_p], c_int),
+    ("cvdvBatchStructSizes", [POINTER(c_int)], None),
+    ("cvdvBatchRunStage", [c_void_p, c_int, c_void_p, c_int, c_void_p, c_int, c_void_p], c_int),
     ("cvdvLaunchCount", [], ctypes.c_ulonglong),
     ("cvdvSetFusion", [c_void_p, c_int], None),
     ("cvdvCancelledTransforms", [c_void_p], ctypes.c_longlong),

@@ -205,6 +205,49 @@ int cvdvBatchCondDispAdjoint(void* psi, void* lam, int precision, int batch, int
 int cvdvBatchOverlap(const void* states, const void* target, int precision, int batch, int n,
                      int targetPerInstance, double* out, void* stream);
 
+/* ---------------------------------------------------------------- batched
+ * independent circuits (no reference counterpart).  Many instances, each with
+ * its own layout [1-qubit registers..., mode of 2^8..2^14 points] and its own
+ * gate list, advance one gate per stage; one persistent launch runs every
+ * instance's gate of a stage.  The host compiles each instance's gate into
+ * tasks: a row program (the mode's transforms and diagonal phases, row by
+ * row) or a qubit pair gate.  Diagonal phases are evaluated in-kernel:
+ *   factor(j) = scale exp(i [tw theta_j + g0 + Z h0 + (a1 + Z b1) x + (a2 + Z b2) x^2 + a3 x^3])
+ * with x = (j - (N-1)/2) dx, theta_j the transform twiddle pi (N-1)(2j-N+1)/(2N),
+ * and Z = -1 when flat bit ctrlBit of the row is set (+1 otherwise or if -1). */
+typedef struct {
+  double a1, b1, a2, b2, a3, g0, h0, scale;
+  int tw;
+  int ctrlBit;
+} CvdvBatchPhase;
+
+typedef struct {
+  int nOps;
+  int op[15]; /* 0 next diagonal phase, 1 forward DFT, 2 inverse DFT (unnormalised), 3 parity */
+  CvdvBatchPhase phase[8];
+} CvdvBatchProgram;
+
+typedef struct {
+  long long stateOffset; /* first amplitude of the instance in the batch array */
+  int kind;              /* 0 row program, 1 2x2 gate on a qubit bit */
+  int n;                 /* qubits of the instance */
+  int logRow;            /* qubits of its mode (row length) */
+  int first;             /* first row (row program) or first pair (gate) */
+  int count;             /* rows or pairs */
+  int bit;               /* gate: flat bit */
+  int program;           /* row program: index into the program table */
+  int pad;
+  double m[8];           /* gate: 2x2 matrix row-major, (re, im) pairs */
+} CvdvBatchTask;
+
+/* sizes[0..2] = sizeof(CvdvBatchPhase), sizeof(CvdvBatchProgram), sizeof(CvdvBatchTask) */
+void cvdvBatchStructSizes(int* sizes);
+/* Run one stage: tasks[0..nTasks) (device) over the batch array `states`
+ * (complex128 or complex64), row programs from `programs` (device), on
+ * gridCtas persistent CTAs of 512 threads; enqueue only. */
+int cvdvBatchRunStage(void* states, int precision, const CvdvBatchTask* tasks, int nTasks,
+                      const CvdvBatchProgram* programs, int gridCtas, void* stream);
+
 /* No counterpart in the reference.  The joint marginal of cvdvMeasureMultiple
  * for callers that cannot let the library allocate device memory (their device
  * memory belongs to another allocator, is fixed at start-up, or must not see

@@ -75,3 +75,12 @@ def test_no_cpu_fallback_in_product():
     for f in os.listdir(pkg):
         if f.endswith(".py"):
             assert "oracle" not in open(os.path.join(pkg, f)).read(), f
+
+
+def test_batch_struct_layouts_match(lib_path):
+    """The numpy record layouts the host builds match the C structs of the stage kernel."""
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "cuda-cvdv_b200"))
+    from cvdv_b200 import batch
+    sizes = batch.struct_sizes()
+    assert sizes == (batch.PHASE_DTYPE.itemsize, batch.PROGRAM_DTYPE.itemsize, batch.TASK_DTYPE.itemsize)
