@@ -354,7 +354,52 @@ struct Op {
   std::vector<Term> pre, post;
   int rowReg = -1;                  // row program on this register when >= 0
   std::vector<HostRowOp> row;
+  bool blockedIn = false, blockedOut = false;
 };
+
+static bool xx_touches(const std::vector<Term>& terms, int r) {
+  for (const Term& t : terms)
+    if (t.kind == kTermXX && (t.r == r || t.s == r)) return true;
+  return false;
+}
+
+// Pair a row program that ends with a forward 2^14-point transform (two-CTA
+// kernel) with the next row program on the same register that starts with the
+// inverse one, when everything in between only reads that register through
+// factor tables (qubit gates, transforms of other registers, diagonal runs
+// without bilinear terms on it).  The pair keeps the register in the blocked
+// order in between, which saves the two layout swaps.
+static void pair_blocked_programs(Context* ctx, std::vector<Op>& ops) {
+  for (size_t i = 0; i < ops.size(); ++i) {
+    Op& a = ops[i];
+    if (a.rowReg < 0 || !rowc_takes(ctx, a.rowReg, a.row)) continue;
+    int lastDir = 0, firstDir = 0;
+    for (const HostRowOp& h : a.row)
+      if (h.kind == kRowFft) lastDir = h.dir;
+    if (lastDir <= 0) continue;
+    const int r = a.rowReg;
+    for (size_t j = i + 1; j < ops.size(); ++j) {
+      Op& b = ops[j];
+      if (b.rowReg == r) {
+        for (const HostRowOp& h : b.row)
+          if (h.kind == kRowFft) {
+            firstDir = h.dir;
+            break;
+          }
+        if (firstDir < 0 && rowc_takes(ctx, r, b.row)) {
+          a.blockedOut = true;
+          b.blockedIn = true;
+          i = j - 1;  // b may itself end forward and pair with a later program
+        }
+        break;
+      }
+      if (b.rowReg >= 0) break;
+      if (b.st && b.st->kind == kStPerm) break;
+      if (b.st && b.st->kind == kStFft && b.st->reg == r) break;
+      if (xx_touches(b.pre, r) || xx_touches(b.post, r)) break;
+    }
+  }
+}
 
 // Number of consecutive pair ops from ops[i] that one qubit-gate sequence can
 // take: at most kSeqMaxBits distinct bits, and every diagonal run among them
@@ -506,6 +551,11 @@ bool flush(Context* ctx) {
       ops.back().post = diag;
     }
   }
+  pair_blocked_programs(ctx, ops);
+  struct PermReset {  // the blocked layout never outlives the flush, errors included
+    Context* c;
+    ~PermReset() { c->permReg = -1; }
+  } permReset{ctx};
   for (size_t oi = 0; oi < ops.size(); ++oi) {
     Op& op = ops[oi];
     if (ctx->fuseSeq && op.st && op.st->kind == kStPair) {
@@ -525,7 +575,12 @@ bool flush(Context* ctx) {
       }
     }
     if (op.rowReg >= 0) {
-      if (!launch_row_program(ctx, op.rowReg, op.row)) return false;
+      if (op.blockedIn) ctx->permReg = -1;  // this program reads the blocked layout itself
+      if (!launch_row_program(ctx, op.rowReg, op.row, op.blockedIn, op.blockedOut)) return false;
+      if (op.blockedOut) {
+        ctx->permReg = op.rowReg;
+        ctx->permLogC = 1;
+      }
       continue;
     }
     if (!op.st) {  // standalone diagonal run

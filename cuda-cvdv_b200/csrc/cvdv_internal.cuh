@@ -259,6 +259,12 @@ struct Context {
   // dropped from the queue.  On by default (cvdvSetFusion).
   bool cancelFt = true;
   bool fuseSeq = true;  // run chains of qubit gates as one qubit-gate sequence pass
+  // Inside one flush, between a forward and an inverse 2^14-point transform of
+  // the last register run by the two-CTA row kernel, that register may be stored
+  // "blocked": position r M + k2 holds logical index r + 2 k2 (the transform's
+  // natural output order).  While permReg >= 0, tables over it are built permuted.
+  int permReg = -1;
+  int permLogC = 0;
   int nextFtTag = 1;
   long long ftCancelled = 0;
 
@@ -323,7 +329,13 @@ struct HostRowOp {
 };
 bool row_eligible(Context* ctx, int reg);
 bool row_diag_fits(Context* ctx, int reg, const std::vector<Term>& terms);
-bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops);
+// blockedIn: the register is stored blocked and the program starts with an
+// inverse transform; blockedOut: leave it blocked after the final forward transform
+bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops, bool blockedIn = false,
+                        bool blockedOut = false);
+// whether launch_row_program runs this program on the two-CTA kernel (which can
+// store and load the blocked layout)
+bool rowc_takes(Context* ctx, int reg, const std::vector<HostRowOp>& ops);
 // qubit-gate sequences (kernels_seq.cu): 2x2 gates on up to four bits and the
 // diagonal runs between them in one pass
 constexpr int kSeqMaxBits = 5;  // complex64; complex128 sequences take at most 4 (seq_max_bits)

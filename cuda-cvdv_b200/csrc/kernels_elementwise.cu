@@ -136,7 +136,8 @@ bool launch_build_table(Context* ctx, int r, bool ctrl, const Term* terms, int n
           !(terms[t].ctrlBit >= lo && terms[t].ctrlBit < hi))
         bit = terms[t].ctrlBit;
   }
-  return launch_build_table_ext(ctx, r, ctrl ? 1 : 0, &bit, terms, nTerms, out);
+  return launch_build_table_ext(ctx, r, ctrl ? 1 : 0, &bit, terms, nTerms, out,
+                                r == ctx->permReg ? ctx->permLogC : 0);
 }
 
 // ----------------------------------------------------------------- diag run

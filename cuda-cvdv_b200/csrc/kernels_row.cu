@@ -79,7 +79,8 @@ struct RowProgram {
   int nOps;
   int nDiag;
   int logTwN;
-  int loadT;    // cluster rows: load (and start) in the transposed layout
+  int loadT;    // cluster rows: start transposed (1: from the natural layout, 2: from the blocked one)
+  int storeBlocked;  // two-CTA rows ending transposed: write the blocked layout
   const double2* tw;
   RowOp ops[kMaxRowOps];
   RowDiag diag[kMaxRowDiags];
@@ -653,7 +654,10 @@ __global__ void __launch_bounds__(1 << (LOGN - 5), 1)
   }
   C v[16];
   bool layoutT = P.loadT != 0;
-  if (!layoutT) {
+  if (P.loadT == 2) {  // blocked: this CTA's X[r + 2 k2] are contiguous at r M + k2
+#pragma unroll
+    for (int w = 0; w < 16; ++w) v[w] = in[rowBase + (uint64_t)r * M + t + TPR * w];
+  } else if (!layoutT) {
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
       v[i] = in[rowBase + t + TPR * (8 * r + i)];
@@ -725,6 +729,9 @@ __global__ void __launch_bounds__(1 << (LOGN - 5), 1)
       out[rowBase + t + TPR * (8 * r + i)] = v[i];
       out[rowBase + M + t + TPR * (8 * r + i)] = v[8 + i];
     }
+  } else if (P.storeBlocked) {
+#pragma unroll
+    for (int w = 0; w < 16; ++w) out[rowBase + (uint64_t)r * M + t + TPR * w] = v[w];
   } else {
     C give[8], got[8];
 #pragma unroll
@@ -863,7 +870,31 @@ static cudaError_t launch_row_t(Context* ctx, const RowProgram& P, uint64_t nCta
   return cudaLaunchKernelEx(&cfg, kern, (const C*)ctx->state(), (C*)ctx->other(), P);
 }
 
-bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops) {
+static bool rowc_shape(Context* ctx, int reg, const std::vector<HostRowOp>& ops) {
+  if (ctx->precision != kC128 || ctx->q[reg] != 14 || !row_eligible(ctx, reg)) return false;
+  int lastDir = 0;
+  for (const HostRowOp& h : ops)
+    if (h.kind == kRowFft) {
+      if (h.dir == lastDir) return false;
+      lastDir = h.dir;
+    }
+  return true;
+}
+
+bool rowc_takes(Context* ctx, int reg, const std::vector<HostRowOp>& ops) {
+  if (!rowc_shape(ctx, reg, ops)) return false;
+  for (const HostRowOp& h : ops) {
+    if (h.kind != kRowDiag) continue;
+    std::vector<Term> regTerms, rowTerms, elemTerms;
+    std::vector<int> bits;
+    if (!split_row_diag(ctx, reg, h.terms, &regTerms, &bits, &rowTerms, &elemTerms) || !elemTerms.empty())
+      return false;
+  }
+  return true;
+}
+
+bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops, bool blockedIn,
+                        bool blockedOut) {
   RowProgram P{};
   // Registers up to the normal tile run two 256-thread CTAs per SM; longer ones
   // use the big tile (512 threads, twice the amplitudes, one CTA per SM) and, past
@@ -934,6 +965,10 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
   }
   bool elemF = false;
   for (int d = 0; d < P.nDiag; ++d) elemF |= P.diag[d].hasElemF != 0;
+  if ((blockedIn || blockedOut) && !(ctx->precision == kC128 && q == 14 && logC == 1 && !elemF)) {
+    set_error(ctx, kErrUnsupported, "blocked layout requested for a program the two-CTA kernel does not run");
+    return false;
+  }
   // the two-CTA kernel needs transforms that alternate in direction (each forward
   // leaves the transposed layout an inverse consumes)
   bool alternating = true;
@@ -944,6 +979,8 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
       lastDir = P.ops[o].dir;
     }
   if (ctx->precision == kC128 && q == 14 && logC == 1 && !elemF && alternating) {
+    if (blockedIn) P.loadT = 2;
+    P.storeBlocked = blockedOut ? 1 : 0;
     cudaError_t er;
     {
       LaunchScope _ls(ctx, kKFft);
