@@ -99,15 +99,23 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+_BACKEND = "nccl"
+
+
 def dist_init():
+    """One process per GPU under torchrun (RANK / LOCAL_RANK / WORLD_SIZE / MASTER_*).
+    NCCL on GPU boxes; gloo where CUDA is absent (the CPU tests of the multi-rank path)."""
+    global _BACKEND
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
         import datetime
 
+        import torch
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        _BACKEND = os.environ.get("CVDV_DIST_BACKEND", "nccl" if torch.cuda.is_available() else "gloo")
+        dist.init_process_group(_BACKEND, timeout=datetime.timedelta(seconds=300))
     return world, rank, local
 
 
@@ -116,7 +124,7 @@ def max_over_ranks(x: float, world: int) -> float:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if _BACKEND == "nccl" else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -169,8 +177,10 @@ def run_reference(args, world, rank):
         return
     from cvdv_b200 import workloads as W
     threads = os.cpu_count() or 1
-    circ = W.state_transfer()
+    circ = W.state_transfer() if args.workload == "full" else W.state_transfer(n_qubits=10)
     # one gate per step, cycling through the circuit; warm-up gates are untimed
+    nq = len(circ["qubits"]) - 1
+    n_tot = sum(circ["qubits"])
     n = args.warmup + args.steps
     times = cpu_oracle_gates(circ, list(range(n)), threads)
     timed = times[args.warmup:]
@@ -181,10 +191,10 @@ def run_reference(args, world, rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sec / len(timed),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
         "data": "synthetic (seeded circuit, seed 2)",
-        "config": {"workload": "state_transfer [1]*14+[14], 2^28 amplitudes, complex128",
+        "config": {"workload": f"state_transfer [1]*{nq}+[14], 2^{n_tot} amplitudes, complex128",
                    "step": "one gate of the circuit (cycling), CPU oracle"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{len(timed)} gates of the 42-gate circuit at full size "
+                         "sample": f"{len(timed)} gates of the {len(circ['gates'])}-gate circuit at 2^{n_tot} "
                                    f"(numpy elementwise single-threaded, scipy FFT on {threads} threads)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }

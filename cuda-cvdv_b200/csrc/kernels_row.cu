@@ -81,6 +81,8 @@ struct RowProgram {
   int logTwN;
   int loadT;    // cluster rows: start transposed (1: from the natural layout, 2: from the blocked one)
   int storeBlocked;  // two-CTA rows ending transposed: write the blocked layout
+  int dualHead;      // two-CTA rows: index of a leading forward transform whose radix-2 step
+                     // reads the whole row in both CTAs (no swap), or -1
   const double2* tw;
   RowOp ops[kMaxRowOps];
   RowDiag diag[kMaxRowDiags];
@@ -658,10 +660,12 @@ __global__ void __launch_bounds__(1 << (LOGN - 5), 1)
 #pragma unroll
     for (int w = 0; w < 16; ++w) v[w] = in[rowBase + (uint64_t)r * M + t + TPR * w];
   } else if (!layoutT) {
+    if (P.dualHead < 0) {
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      v[i] = in[rowBase + t + TPR * (8 * r + i)];
-      v[8 + i] = in[rowBase + M + t + TPR * (8 * r + i)];
+      for (int i = 0; i < 8; ++i) {
+        v[i] = in[rowBase + t + TPR * (8 * r + i)];
+        v[8 + i] = in[rowBase + M + t + TPR * (8 * r + i)];
+      }
     }
   } else {
     // pairs X[2 k2], X[2 k2 + 1] for k2 in this CTA's half; keep X[r + 2 k2]
@@ -682,7 +686,57 @@ __global__ void __launch_bounds__(1 << (LOGN - 5), 1)
   }
   __syncthreads();  // twiddle tables
 
-  for (int o = 0; o < P.nOps; ++o) {
+  int o0 = 0;
+  if (P.dualHead >= 0) {
+    // Leading forward transform: both CTAs read the whole row (the second read of
+    // each element comes from L2) and form y_r[m] = w_N^{m r} (x[m] + (-1)^r x[M + m])
+    // for all 16 of their m directly, after the leading diagonal runs.
+    double2 rs[2];
+    int seg[2];
+    for (int o = 0; o < P.dualHead; ++o) {
+      const RowDiag& D = P.diag[P.ops[o].diag];
+      rs[o] = D.hasRowF ? eval_factor(D.rowF, rowBase) : make_double2(1.0, 0.0);
+      int sg = 0;
+      for (int c = 0; c < D.nCtrl; ++c) sg |= (int)((rowBase >> D.ctrlShift[c]) & 1ull) << c;
+      seg[o] = sg << LOGN;
+    }
+#pragma unroll
+    for (int w0 = 0; w0 < 16; w0 += 4) {
+      C a[4], b[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int m = t + TPR * (w0 + j);
+        a[j] = in[rowBase + m];
+        b[j] = in[rowBase + M + m];
+      }
+      for (int o = 0; o < P.dualHead; ++o) {
+        const RowDiag& D = P.diag[P.ops[o].diag];
+        if (!D.tab && !D.hasRowF) continue;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int m = t + TPR * (w0 + j);
+          double2 fa = D.tab ? __ldg(D.tab + seg[o] + m) : make_double2(1.0, 0.0);
+          double2 fb = D.tab ? __ldg(D.tab + seg[o] + M + m) : make_double2(1.0, 0.0);
+          if (D.hasRowF) {
+            fa = dmul(fa, rs[o]);
+            fb = dmul(fb, rs[o]);
+          }
+          a[j] = cmul(a[j], fromd<C>(fa));
+          b[j] = cmul(b[j], fromd<C>(fb));
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int m = t + TPR * (w0 + j);
+        v[w0 + j] = r ? cmul(csub(a[j], b[j]), tw2<C, 1>(loN, hiN, m)) : cadd(a[j], b[j]);
+      }
+    }
+    rr_stages<C, 1, LOGM, 0, 4>(v, sm, t, loM, hiM);
+    layoutT = true;
+    o0 = P.dualHead + 1;
+  }
+
+  for (int o = o0; o < P.nOps; ++o) {
     const RowOp& op = P.ops[o];
     if (op.kind == kRowDiag) {
       rc_diag<C, LOGM>(v, P.diag[op.diag], rowBase, t, r, layoutT);
@@ -981,6 +1035,12 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
   if (ctx->precision == kC128 && q == 14 && logC == 1 && !elemF && alternating) {
     if (blockedIn) P.loadT = 2;
     P.storeBlocked = blockedOut ? 1 : 0;
+    P.dualHead = -1;
+    if (P.loadT == 0) {
+      int f = 0;
+      while (f < P.nOps && P.ops[f].kind == kRowDiag) ++f;
+      if (f < P.nOps && f <= 2 && P.ops[f].dir > 0) P.dualHead = f;
+    }
     cudaError_t er;
     {
       LaunchScope _ls(ctx, kKFft);
