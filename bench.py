@@ -277,6 +277,14 @@ def run_gpu(args, world, rank, local):
 
     kr = kern_roof(stats, alg_bytes)
     dom = max(kr, key=lambda k: kr[k]["share_of_kernel_time"])
+    # DRAM bytes (read + write) per launch from ncu captures of the same kernels on the
+    # 2^24-amplitude version of this workload (profiles/*_state_transfer_2p24.md),
+    # scaled by the 16x larger state: the kernels stream the state once per launch,
+    # so their traffic grows with the rows / sites processed.
+    ncu_traffic_2p24 = {"fft_pass": ((269.3 + 219.8) + (269.1 + 222.2)) / 2 * 1e6,  # k_rowc, two launches
+                        "seq": (269.5 + 209.9) * 1e6}                                  # k_seq<double2, 2>
+    scale = n_amp / float(1 << 24)
+    traffic = ncu_traffic_2p24[dom] * scale if (dom in ncu_traffic_2p24 and args.workload == "full") else None
     achieved = kr[dom]["achieved_gbs"]
     value = G * world / (ms * 1e-3)
 
@@ -324,7 +332,9 @@ def run_gpu(args, world, rank, local):
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "kernel": KNAME[dom],
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "peak_kind": peak_kind, "traffic": None,
+                     "peak_kind": peak_kind, "traffic": traffic,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the 2^24 capture "
+                                       "in profiles/, x16 (writes still in L2 at kernel end are not counted)",
                      "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": kr[dom]["avg_launch_ms"],
                      "launches": kr[dom]["launches"], "share_of_kernel_time": kr[dom]["share_of_kernel_time"],
                      "kernels": kr},
