@@ -338,7 +338,7 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
 bool rowc_takes(Context* ctx, int reg, const std::vector<HostRowOp>& ops);
 // qubit-gate sequences (kernels_seq.cu): 2x2 gates on up to four bits and the
 // diagonal runs between them in one pass
-constexpr int kSeqMaxBits = 5;  // complex64; complex128 sequences take at most 4 (seq_max_bits)
+constexpr int kSeqMaxBits = 5;  // see seq_max_bits
 constexpr int kSeqMaxOps = 24;
 constexpr int kSeqMaxDiags = 10;
 constexpr int kSeqMaxTabs = 4;

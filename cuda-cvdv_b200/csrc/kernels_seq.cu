@@ -105,28 +105,75 @@ __device__ __forceinline__ void seq_scale(C* v, double2 f0, double2 f1) {
 #define SEQ_BIT_SWITCH(b, CALL)                          \
   switch (b) {                                           \
     case 0: { constexpr int B_ = 0; CALL; } break;       \
-    case 1: if constexpr (NB > 1) { constexpr int B_ = 1; CALL; } break; \
-    case 2: if constexpr (NB > 2) { constexpr int B_ = 2; CALL; } break; \
-    case 3: if constexpr (NB > 3) { constexpr int B_ = 3; CALL; } break; \
-    default: if constexpr (NB > 4) { constexpr int B_ = 4; CALL; } break; \
+    case 1: if constexpr (NBL > 1) { constexpr int B_ = 1; CALL; } break; \
+    case 2: if constexpr (NBL > 2) { constexpr int B_ = 2; CALL; } break; \
+    case 3: if constexpr (NBL > 3) { constexpr int B_ = 3; CALL; } break; \
+    default: if constexpr (NBL > 4) { constexpr int B_ = 4; CALL; } break; \
   }
 
-template <typename C, int NB, typename IDX>
+template <typename C> __device__ __forceinline__ C shfl_xor_c(C v, int m);
+template <> __device__ __forceinline__ double2 shfl_xor_c<double2>(double2 v, int m) {
+  return make_double2(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
+}
+template <> __device__ __forceinline__ float2 shfl_xor_c<float2>(float2 v, int m) {
+  return make_float2(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
+}
+
+// 2x2 gate on a bit split across lanes: the partner amplitude (same local index)
+// lives in lane ^ lm; `hi` is this lane's value of the bit
+template <typename C, int KL>
+__device__ __forceinline__ void seq_pair_lanes(C* v, int kind, const double2* m, int lm, int hi) {
+  using R = typename SeqReal<C>::t;
+  if (kind == kSeqPairH) {
+#pragma unroll
+    for (int k = 0; k < KL; ++k) {
+      const C o = shfl_xor_c(v[k], lm);
+      v[k] = hi ? csub(o, v[k]) : cadd(v[k], o);
+    }
+  } else if (kind == kSeqPairReal) {
+    const R c0 = (R)(hi ? m[2].x : m[0].x), c1 = (R)(hi ? m[3].x : m[1].x);
+#pragma unroll
+    for (int k = 0; k < KL; ++k) {
+      const C o = shfl_xor_c(v[k], lm);
+      const C x0 = hi ? o : v[k], x1 = hi ? v[k] : o;
+      v[k] = mk(c0 * x0.x + c1 * x1.x, c0 * x0.y + c1 * x1.y);
+    }
+  } else {
+    const C c0 = fromd<C>(hi ? m[2] : m[0]), c1 = fromd<C>(hi ? m[3] : m[1]);
+#pragma unroll
+    for (int k = 0; k < KL; ++k) {
+      const C o = shfl_xor_c(v[k], lm);
+      const C x0 = hi ? o : v[k], x1 = hi ? v[k] : o;
+      v[k] = cadd(cmul(c0, x0), cmul(c1, x1));
+    }
+  }
+}
+
+// A site of 2^NB amplitudes is held by 2^SPLIT consecutive lanes: the top SPLIT
+// selected bits pick the lane, the other NB - SPLIT the register.  Gates on a
+// lane bit exchange partners with warp shuffles.
+template <typename C, int NB, int SPLIT, typename IDX>
 __global__ void __launch_bounds__(256, 2) k_seq(C* __restrict__ st, IDX nSites,
                                                const __grid_constant__ SeqProgram P) {
-  constexpr int K = 1 << NB;
+  constexpr int NBL = NB - SPLIT;  // bits held in registers
+  constexpr int KL = 1 << NBL;
   using R = typename SeqReal<C>::t;
-  // offsets of a site's amplitudes from its base (the same for every site),
-  // kept in shared memory rather than in 2^NB registers per thread
-  __shared__ IDX soff[K];
-  if (threadIdx.x < K) {
+  // offsets of a site's register amplitudes from its base (the same for every
+  // site), kept in shared memory rather than in 2^NBL registers per thread
+  __shared__ IDX soff[KL];
+  if (threadIdx.x < KL) {
     IDX o = 0;
-    for (int b = 0; b < NB; ++b)
+    for (int b = 0; b < NBL; ++b)
       if (threadIdx.x & (1u << b)) o += (IDX)1 << P.bits[b];
     soff[threadIdx.x] = o;
   }
   __syncthreads();
-  for (IDX s = (IDX)blockIdx.x * blockDim.x + threadIdx.x; s < nSites; s += (IDX)gridDim.x * blockDim.x) {
+  // every lane of a site runs every iteration: total is a multiple of the warp
+  // size (the host keeps 2^(n - NB + SPLIT) >= 32 when SPLIT > 0)
+  const IDX total = nSites << SPLIT;
+  for (IDX g = (IDX)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += (IDX)gridDim.x * blockDim.x) {
+    const IDX s = g >> SPLIT;
+    const int part = (int)(g & (IDX)((1 << SPLIT) - 1));
     // site base: s with a zero inserted at every selected bit (ascending order)
     IDX base = s;
 #pragma unroll
@@ -134,19 +181,28 @@ __global__ void __launch_bounds__(256, 2) k_seq(C* __restrict__ st, IDX nSites,
       const IDX low = ((IDX)1 << P.bits[b]) - 1;
       base = ((base & ~low) << 1) | (base & low);
     }
-    C v[K];
+    IDX hoff = 0;
 #pragma unroll
-    for (int k = 0; k < K; ++k) v[k] = st[base + soff[k]];
+    for (int i = 0; i < SPLIT; ++i)
+      if ((part >> i) & 1) hoff += (IDX)1 << P.bits[NBL + i];
+    C v[KL];
+#pragma unroll
+    for (int k = 0; k < KL; ++k) v[k] = st[base + hoff + soff[k]];
     R sc = (R)1;  // pending real factor of Hadamard-type pairs
     for (int o = 0; o < P.nOps; ++o) {
       const SeqOp& op = P.ops[o];
-      if (op.kind == kSeqPairH) {
-        sc *= (R)op.m[0].x;
-        SEQ_BIT_SWITCH(op.bit, (seq_pair_h<C, NB, B_>(v)))
-      } else if (op.kind == kSeqPairReal) {
-        SEQ_BIT_SWITCH(op.bit, (seq_pair_real<C, NB, B_>(v, op.m)))
-      } else if (op.kind == kSeqPair) {
-        SEQ_BIT_SWITCH(op.bit, (seq_pair<C, NB, B_>(v, op.m)))
+      if (op.kind != kSeqDiag) {
+        if (op.kind == kSeqPairH) sc *= (R)op.m[0].x;
+        if (SPLIT > 0 && op.bit >= NBL) {
+          const int lb = op.bit - NBL;
+          seq_pair_lanes<C, KL>(v, op.kind, op.m, 1 << lb, (part >> lb) & 1);
+        } else if (op.kind == kSeqPairH) {
+          SEQ_BIT_SWITCH(op.bit, (seq_pair_h<C, NBL, B_>(v)))
+        } else if (op.kind == kSeqPairReal) {
+          SEQ_BIT_SWITCH(op.bit, (seq_pair_real<C, NBL, B_>(v, op.m)))
+        } else {
+          SEQ_BIT_SWITCH(op.bit, (seq_pair<C, NBL, B_>(v, op.m)))
+        }
       } else {
         const SeqDiag& D = P.diag[op.diag];
         double2 w0 = D.scalar, w1 = D.scalar;
@@ -163,21 +219,22 @@ __global__ void __launch_bounds__(256, 2) k_seq(C* __restrict__ st, IDX nSites,
         w0 = make_double2(w0.x * dsc, w0.y * dsc);
         w1 = make_double2(w1.x * dsc, w1.y * dsc);
         sc = (R)1;
-        if (D.g < 0) {
-          const C c = fromd<C>(w0);
+        if (D.g < 0 || (SPLIT > 0 && D.g >= NBL)) {
+          // the factor does not vary over this lane's registers
+          const C c = fromd<C>((D.g >= 0 && ((part >> (D.g - NBL)) & 1)) ? w1 : w0);
 #pragma unroll
-          for (int k = 0; k < K; ++k) v[k] = cmul(v[k], c);
+          for (int k = 0; k < KL; ++k) v[k] = cmul(v[k], c);
         } else {
-          SEQ_BIT_SWITCH(D.g, (seq_scale<C, NB, B_>(v, w0, w1)))
+          SEQ_BIT_SWITCH(D.g, (seq_scale<C, NBL, B_>(v, w0, w1)))
         }
       }
     }
     if (sc != (R)1) {
 #pragma unroll
-      for (int k = 0; k < K; ++k) v[k] = mk(v[k].x * sc, v[k].y * sc);
+      for (int k = 0; k < KL; ++k) v[k] = mk(v[k].x * sc, v[k].y * sc);
     }
 #pragma unroll
-    for (int k = 0; k < K; ++k) st[base + soff[k]] = v[k];
+    for (int k = 0; k < KL; ++k) st[base + hoff + soff[k]] = v[k];
   }
 }
 
@@ -225,22 +282,37 @@ bool seq_diag_ok(Context* ctx, const std::vector<int>& bits, const std::vector<T
   return tables <= kSeqMaxTabs;
 }
 
-int seq_max_bits(Context* ctx) { return ctx->precision == kC128 ? 4 : 5; }
+// Bits per sequence: 16 (complex128) or 32 (complex64) amplitudes per thread;
+// complex128 sequences of five bits split each site over 2 lanes when the state
+// is large enough that every warp holds whole sites (2^(n - NB + SPLIT) >= 32).
+// (Splitting complex64 sites over 2 or 4 lanes for 6-7 bits measured slower per
+// pass than the extra pass it saves, so complex64 stops at 5.)
+int seq_max_bits(Context* ctx) {
+  if (ctx->precision == kC128) return ctx->totalQbt >= 9 ? 5 : 4;
+  return 5;
+}
+
+template <typename C, int NB, int SPLIT, typename IDX>
+static void seq_go(Context* ctx, unsigned blocks, uint64_t nSites, const SeqProgram& P) {
+  k_seq<C, NB, SPLIT, IDX><<<blocks, 256, 0, ctx->stream>>>((C*)ctx->state(), (IDX)nSites, P);
+}
 
 template <typename C, typename IDX>
 static void seq_dispatch(Context* ctx, int nb, unsigned blocks, uint64_t nSites, const SeqProgram& P) {
-  C* st = (C*)ctx->state();
-  const IDX n = (IDX)nSites;
   switch (nb) {
-    case 1: k_seq<C, 1, IDX><<<blocks, 256, 0, ctx->stream>>>(st, n, P); break;
-    case 2: k_seq<C, 2, IDX><<<blocks, 256, 0, ctx->stream>>>(st, n, P); break;
-    case 3: k_seq<C, 3, IDX><<<blocks, 256, 0, ctx->stream>>>(st, n, P); break;
-    case 4: k_seq<C, 4, IDX><<<blocks, 256, 0, ctx->stream>>>(st, n, P); break;
+    case 1: seq_go<C, 1, 0, IDX>(ctx, blocks, nSites, P); break;
+    case 2: seq_go<C, 2, 0, IDX>(ctx, blocks, nSites, P); break;
+    case 3: seq_go<C, 3, 0, IDX>(ctx, blocks, nSites, P); break;
+    case 4: seq_go<C, 4, 0, IDX>(ctx, blocks, nSites, P); break;
     default:
-      if constexpr (sizeof(C) == sizeof(float2)) k_seq<C, 5, IDX><<<blocks, 256, 0, ctx->stream>>>(st, n, P);
+      if constexpr (sizeof(C) == sizeof(float2)) seq_go<C, 5, 0, IDX>(ctx, blocks, nSites, P);
+      else seq_go<C, 5, 1, IDX>(ctx, blocks, nSites, P);
       break;
   }
 }
+
+// lanes per site of the kernel seq_dispatch picks
+static int seq_split(Context* ctx, int nb) { return (ctx->precision == kC128 && nb >= 5) ? 1 : 0; }
 
 bool launch_seq(Context* ctx, const std::vector<HostSeqOp>& ops) {
   std::vector<int> bits;
@@ -311,7 +383,7 @@ bool launch_seq(Context* ctx, const std::vector<HostSeqOp>& ops) {
     o.diag = nd++;
   }
   const uint64_t nSites = ctx->size() >> nb;
-  uint64_t blocks = (nSites + 255) / 256;
+  uint64_t blocks = ((nSites << seq_split(ctx, nb)) + 255) / 256;
   if (blocks > 148ull * 8) blocks = 148ull * 8;
   const bool narrow = ctx->totalQbt <= 31;  // every flat index fits 32 bits
   {

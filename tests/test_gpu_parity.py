@@ -308,10 +308,10 @@ def test_qubit_gate_sequences(qubits):
     assert rel(states[("complex128", 3)], states[("complex128", 1)]) < 1e-12
 
 
-@pytest.mark.parametrize("precision,passes", [("complex128", 4), ("complex64", 3)])
+@pytest.mark.parametrize("precision,passes", [("complex128", 3), ("complex64", 3)])
 def test_state_transfer_uses_sequences(precision, passes):
     """The headline chain H . CPhaseX . Rz over 14 qubits runs as a few sequence
-    passes (four qubits each in complex128, five in complex64) between the two
+    passes (five qubits each) between the two
     mode transforms, with the first H moved past the forward transform."""
     from cvdv_b200 import CudaCvdv, _lib
     from cvdv_b200 import workloads as W
