@@ -565,11 +565,12 @@ static cudaError_t launch_rowr(Context* ctx, const RowProgram& P, int q) {
 }
 
 // ---------------------------------------------------------------- two-CTA register-resident rows
-// A row of N = 2 M points (2^14 complex128) is split over a cluster of two CTAs
-// of M/16 threads; every thread keeps 16 amplitudes in registers.  With
-// m_i = t + TPR (8 r + i), i < 8, for thread t of CTA r, two layouts occur:
-//   S ("split natural"): v[i] = x[m_i], v[8 + i] = x[M + m_i];
-//   T ("transposed"):    v[w] = X[r + 2 k2] at k2 = t + TPR w (all 16 w).
+// A row of N = 2 M points (2^14) is split over a cluster of two CTAs of M/E
+// threads; every thread keeps E amplitudes in registers (E = 16 complex128,
+// 32 complex64).  With H = E/2 and m_i = t + TPR (H r + i), i < H, for thread t
+// of CTA r, two layouts occur:
+//   S ("split natural"): v[i] = x[m_i], v[H + i] = x[M + m_i];
+//   T ("transposed"):    v[w] = X[r + 2 k2] at k2 = t + TPR w (all E w).
 // Forward DFT, S -> T:  y_k1[m] = w_N^{m k1} (x[m] + (-1)^k1 x[M + m]); each CTA
 //   forms both y_0 and y_1 on its own m_i, keeps y_r and hands y_(1-r) to the
 //   sibling through distributed shared memory (8 values per thread); then an
@@ -585,36 +586,36 @@ static cudaError_t launch_rowr(Context* ctx, const RowProgram& P, int q) {
 // Hand the sibling 8 registers and take 8 of its: this CTA writes its registers
 // SEND_HI (w = 8 SEND_HI + i) at their canonical positions, the sibling does the
 // same, and each reads the other's.  Both CTAs call it with mirrored halves.
-template <typename C, int TPR>
-__device__ __forceinline__ void rc_swap(C* sm, const C* peer, int t, const C (&send)[8], C (&recv)[8],
+template <typename C, int TPR, int H>
+__device__ __forceinline__ void rc_swap(C* sm, const C* peer, int t, const C (&send)[H], C (&recv)[H],
                                        int sendHalf, int recvHalf) {
   cg::cluster_group cl = cg::this_cluster();
 #pragma unroll
-  for (int i = 0; i < 8; ++i) sm[rpad<C>(t + TPR * (8 * sendHalf + i))] = send[i];
+  for (int i = 0; i < H; ++i) sm[rpad<C>(t + TPR * (H * sendHalf + i))] = send[i];
   cl.sync();
 #pragma unroll
-  for (int i = 0; i < 8; ++i) recv[i] = peer[rpad<C>(t + TPR * (8 * recvHalf + i))];
+  for (int i = 0; i < H; ++i) recv[i] = peer[rpad<C>(t + TPR * (H * recvHalf + i))];
   cl.sync();  // the sibling has read this CTA's buffer before it is reused
 }
 
-template <typename C, int LOGM>
-__device__ __forceinline__ void rc_diag(C (&v)[16], const RowDiag& D, uint64_t rowBase, int t, int r,
+template <typename C, int LOGM, int LOGE>
+__device__ __forceinline__ void rc_diag(C (&v)[1 << LOGE], const RowDiag& D, uint64_t rowBase, int t, int r,
                                         bool layoutT) {
-  constexpr int TPR = 1 << (LOGM - 4), M = 1 << LOGM;
+  constexpr int E = 1 << LOGE, H = E / 2, TPR = 1 << (LOGM - LOGE), M = 1 << LOGM;
   const double2 rs = D.hasRowF ? eval_factor(D.rowF, rowBase) : make_double2(1.0, 0.0);
   if (D.tab) {
     int seg = 0;
     for (int c = 0; c < D.nCtrl; ++c) seg |= (int)((rowBase >> D.ctrlShift[c]) & 1ull) << c;
     const double2* tp = D.tab + ((size_t)seg << (LOGM + 1));
-    // T: permuted table, index r M + k2; S: natural, index (w >> 3) M + m_(w & 7)
-    const double2* base = layoutT ? tp + r * M + t : tp + t + TPR * 8 * r;
+    // T: permuted table, index r M + k2; S: natural, index (w / H) M + m_(w % H)
+    const double2* base = layoutT ? tp + r * M + t : tp + t + TPR * H * r;
 #pragma unroll
-    for (int k0 = 0; k0 < 16; k0 += 8) {
+    for (int k0 = 0; k0 < E; k0 += 8) {
       double2 w[8];
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
         const int kk = k0 + k;
-        w[k] = __ldg(base + (layoutT ? TPR * kk : (kk >> 3) * M + TPR * (kk & 7)));
+        w[k] = __ldg(base + (layoutT ? TPR * kk : (kk / H) * M + TPR * (kk % H)));
       }
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
@@ -625,14 +626,17 @@ __device__ __forceinline__ void rc_diag(C (&v)[16], const RowDiag& D, uint64_t r
   } else if (D.hasRowF) {
     const C c = fromd<C>(rs);
 #pragma unroll
-    for (int k = 0; k < 16; ++k) v[k] = cmul(v[k], c);
+    for (int k = 0; k < E; ++k) v[k] = cmul(v[k], c);
   }
 }
 
-template <typename C, int LOGN>
-__global__ void __launch_bounds__(1 << (LOGN - 5), 1)
+// LOGE: log2 amplitudes per thread (16 for complex128: 512 threads, one CTA per
+// SM; 32 for complex64: 256 threads, two CTAs per SM)
+template <typename C, int LOGN, int LOGE>
+__global__ void __launch_bounds__(1 << (LOGN - 1 - LOGE), (LOGN - 1 - LOGE) > 8 ? 1 : 2)
     k_rowc(const C* __restrict__ in, C* __restrict__ out, const __grid_constant__ RowProgram P) {
-  constexpr int LOGM = LOGN - 1, M = 1 << LOGM, TPR = M >> 4, RS = M + (M >> 4);
+  constexpr int LOGM = LOGN - 1, M = 1 << LOGM, E = 1 << LOGE, H = E / 2, TPR = M >> LOGE;
+  constexpr int RS = M + (M >> 4);
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
   double2* loM = reinterpret_cast<double2*>(sm + RS);  // w_M^e, e < 64
@@ -654,34 +658,34 @@ __global__ void __launch_bounds__(1 << (LOGN - 5), 1)
       loM[i] = __ldg(P.tw + ((size_t)e << (half ? scN : scM)));  // loM..hiN are one array
     }
   }
-  C v[16];
+  C v[E];
   bool layoutT = P.loadT != 0;
   if (P.loadT == 2) {  // blocked: this CTA's X[r + 2 k2] are contiguous at r M + k2
 #pragma unroll
-    for (int w = 0; w < 16; ++w) v[w] = in[rowBase + (uint64_t)r * M + t + TPR * w];
+    for (int w = 0; w < E; ++w) v[w] = in[rowBase + (uint64_t)r * M + t + TPR * w];
   } else if (!layoutT) {
     if (P.dualHead < 0) {
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        v[i] = in[rowBase + t + TPR * (8 * r + i)];
-        v[8 + i] = in[rowBase + M + t + TPR * (8 * r + i)];
+      for (int i = 0; i < H; ++i) {
+        v[i] = in[rowBase + t + TPR * (H * r + i)];
+        v[H + i] = in[rowBase + M + t + TPR * (H * r + i)];
       }
     }
   } else {
     // pairs X[2 k2], X[2 k2 + 1] for k2 in this CTA's half; keep X[r + 2 k2]
-    C keep[8], give[8], got[8];
+    C keep[H], give[H], got[H];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const uint64_t k2 = (uint64_t)(t + TPR * (8 * r + i));
+    for (int i = 0; i < H; ++i) {
+      const uint64_t k2 = (uint64_t)(t + TPR * (H * r + i));
       const C a = in[rowBase + 2 * k2], b = in[rowBase + 2 * k2 + 1];
       keep[i] = r ? b : a;
       give[i] = r ? a : b;
     }
-    rc_swap<C, TPR>(sm, peer, t, give, got, r, r ^ 1);
+    rc_swap<C, TPR, H>(sm, peer, t, give, got, r, r ^ 1);
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      v[r ? 8 + i : i] = keep[i];
-      v[r ? i : 8 + i] = got[i];
+    for (int i = 0; i < H; ++i) {
+      v[r ? H + i : i] = keep[i];
+      v[r ? i : H + i] = got[i];
     }
   }
   __syncthreads();  // twiddle tables
@@ -701,7 +705,7 @@ __global__ void __launch_bounds__(1 << (LOGN - 5), 1)
       seg[o] = sg << LOGN;
     }
 #pragma unroll
-    for (int w0 = 0; w0 < 16; w0 += 4) {
+    for (int w0 = 0; w0 < E; w0 += 4) {
       C a[4], b[4];
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
@@ -731,7 +735,7 @@ __global__ void __launch_bounds__(1 << (LOGN - 5), 1)
         v[w0 + j] = r ? cmul(csub(a[j], b[j]), tw2<C, 1>(loN, hiN, m)) : cadd(a[j], b[j]);
       }
     }
-    rr_stages<C, 1, LOGM, 0, 4>(v, sm, t, loM, hiM);
+    rr_stages<C, 1, LOGM, 0, LOGE>(v, sm, t, loM, hiM);
     layoutT = true;
     o0 = P.dualHead + 1;
   }
@@ -739,39 +743,39 @@ __global__ void __launch_bounds__(1 << (LOGN - 5), 1)
   for (int o = o0; o < P.nOps; ++o) {
     const RowOp& op = P.ops[o];
     if (op.kind == kRowDiag) {
-      rc_diag<C, LOGM>(v, P.diag[op.diag], rowBase, t, r, layoutT);
+      rc_diag<C, LOGM, LOGE>(v, P.diag[op.diag], rowBase, t, r, layoutT);
     } else if (op.dir > 0) {  // S -> T
-      C mine[8], give[8], got[8];
+      C mine[H], give[H], got[H];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const int m = t + TPR * (8 * r + i);
-        const C a = v[i], b = v[8 + i];
+      for (int i = 0; i < H; ++i) {
+        const int m = t + TPR * (H * r + i);
+        const C a = v[i], b = v[H + i];
         const C y0 = cadd(a, b);
         const C y1 = cmul(csub(a, b), tw2<C, 1>(loN, hiN, m));
         mine[i] = r ? y1 : y0;
         give[i] = r ? y0 : y1;
       }
-      rc_swap<C, TPR>(sm, peer, t, give, got, r, r ^ 1);
+      rc_swap<C, TPR, H>(sm, peer, t, give, got, r, r ^ 1);
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        v[r ? 8 + i : i] = mine[i];
-        v[r ? i : 8 + i] = got[i];
+      for (int i = 0; i < H; ++i) {
+        v[r ? H + i : i] = mine[i];
+        v[r ? i : H + i] = got[i];
       }
-      rr_stages<C, 1, LOGM, 0, 4>(v, sm, t, loM, hiM);
+      rr_stages<C, 1, LOGM, 0, LOGE>(v, sm, t, loM, hiM);
       layoutT = true;
     } else {  // T -> S
-      rr_stages<C, -1, LOGM, 0, 4>(v, sm, t, loM, hiM);
-      C give[8], got[8];
+      rr_stages<C, -1, LOGM, 0, LOGE>(v, sm, t, loM, hiM);
+      C give[H], got[H];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) give[i] = v[r ? i : 8 + i];  // the sibling's half of z_r
-      rc_swap<C, TPR>(sm, peer, t, give, got, r ^ 1, r);
+      for (int i = 0; i < H; ++i) give[i] = v[r ? i : H + i];  // the sibling's half of z_r
+      rc_swap<C, TPR, H>(sm, peer, t, give, got, r ^ 1, r);
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const int m = t + TPR * (8 * r + i);
+      for (int i = 0; i < H; ++i) {
+        const int m = t + TPR * (H * r + i);
         const C z0 = r ? got[i] : v[i];
-        const C z1 = cmul(r ? v[8 + i] : got[i], tw2<C, -1>(loN, hiN, m));
+        const C z1 = cmul(r ? v[H + i] : got[i], tw2<C, -1>(loN, hiN, m));
         v[i] = cadd(z0, z1);
-        v[8 + i] = csub(z0, z1);
+        v[H + i] = csub(z0, z1);
       }
       layoutT = false;
     }
@@ -779,38 +783,38 @@ __global__ void __launch_bounds__(1 << (LOGN - 5), 1)
 
   if (!layoutT) {
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      out[rowBase + t + TPR * (8 * r + i)] = v[i];
-      out[rowBase + M + t + TPR * (8 * r + i)] = v[8 + i];
+    for (int i = 0; i < H; ++i) {
+      out[rowBase + t + TPR * (H * r + i)] = v[i];
+      out[rowBase + M + t + TPR * (H * r + i)] = v[H + i];
     }
   } else if (P.storeBlocked) {
 #pragma unroll
-    for (int w = 0; w < 16; ++w) out[rowBase + (uint64_t)r * M + t + TPR * w] = v[w];
+    for (int w = 0; w < E; ++w) out[rowBase + (uint64_t)r * M + t + TPR * w] = v[w];
   } else {
-    C give[8], got[8];
+    C give[H], got[H];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) give[i] = v[r ? i : 8 + i];  // X[r + 2 k2] for the sibling's k2
-    rc_swap<C, TPR>(sm, peer, t, give, got, r ^ 1, r);
+    for (int i = 0; i < H; ++i) give[i] = v[r ? i : H + i];  // X[r + 2 k2] for the sibling's k2
+    rc_swap<C, TPR, H>(sm, peer, t, give, got, r ^ 1, r);
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const uint64_t k2 = (uint64_t)(t + TPR * (8 * r + i));
-      const C own = v[r ? 8 + i : i];
+    for (int i = 0; i < H; ++i) {
+      const uint64_t k2 = (uint64_t)(t + TPR * (H * r + i));
+      const C own = v[r ? H + i : i];
       out[rowBase + 2 * k2] = r ? got[i] : own;
       out[rowBase + 2 * k2 + 1] = r ? own : got[i];
     }
   }
 }
 
-template <typename C, int LOGN>
+template <typename C, int LOGN, int LOGE>
 static cudaError_t launch_rowc_t(Context* ctx, const RowProgram& P) {
   constexpr int M = 1 << (LOGN - 1);
   const size_t smem = (size_t)(M + (M >> 4)) * sizeof(C) + 2 * (64 + (M >> 6)) * sizeof(double2);
-  auto kern = k_rowc<C, LOGN>;
+  auto kern = k_rowc<C, LOGN, LOGE>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3((unsigned)(ctx->size() >> (LOGN - 1)));
-  cfg.blockDim = dim3(M >> 4);
+  cfg.blockDim = dim3(M >> LOGE);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = ctx->stream;
   cudaLaunchAttribute attr[1];
@@ -924,6 +928,9 @@ static cudaError_t launch_row_t(Context* ctx, const RowProgram& P, uint64_t nCta
   return cudaLaunchKernelEx(&cfg, kern, (const C*)ctx->state(), (C*)ctx->other(), P);
 }
 
+// 2^14-point complex128 rows run on the two-CTA kernel.  (Complex64 rows of that
+// length fit one CTA, k_rowr; the two-CTA form with two 256-thread CTAs per SM
+// measured slower for them: the half swaps cost more than the overlap gains.)
 static bool rowc_shape(Context* ctx, int reg, const std::vector<HostRowOp>& ops) {
   if (ctx->precision != kC128 || ctx->q[reg] != 14 || !row_eligible(ctx, reg)) return false;
   int lastDir = 0;
@@ -957,6 +964,8 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
   int logT = q <= row_log_tile(ctx->precision) ? 8 : 9;
   int lt = row_log_tile(ctx->precision) + (logT - 8);
   int logC = q > lt ? q - lt : 0;
+  const bool useC = rowc_takes(ctx, reg, ops);  // the two-CTA register-resident kernel
+  if (useC) logC = 1;
   P.logN = q;
   P.logM = q - logC;
   P.logRows = q < lt ? lt - q : 0;
@@ -1019,7 +1028,7 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
   }
   bool elemF = false;
   for (int d = 0; d < P.nDiag; ++d) elemF |= P.diag[d].hasElemF != 0;
-  if ((blockedIn || blockedOut) && !(ctx->precision == kC128 && q == 14 && logC == 1 && !elemF)) {
+  if ((blockedIn || blockedOut) && !useC) {
     set_error(ctx, kErrUnsupported, "blocked layout requested for a program the two-CTA kernel does not run");
     return false;
   }
@@ -1032,7 +1041,7 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
       alternating &= P.ops[o].dir != lastDir;
       lastDir = P.ops[o].dir;
     }
-  if (ctx->precision == kC128 && q == 14 && logC == 1 && !elemF && alternating) {
+  if (useC && !elemF && alternating) {
     if (blockedIn) P.loadT = 2;
     P.storeBlocked = blockedOut ? 1 : 0;
     P.dualHead = -1;
@@ -1044,7 +1053,7 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
     cudaError_t er;
     {
       LaunchScope _ls(ctx, kKFft);
-      er = launch_rowc_t<double2, 14>(ctx, P);
+      er = launch_rowc_t<double2, 14, 4>(ctx, P);
     }
     if (!cuda_ok(ctx, er, "row program launch")) return false;
     ctx->cur ^= 1;
