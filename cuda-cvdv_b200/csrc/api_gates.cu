@@ -304,6 +304,11 @@ CVDVContext* cvdvCreateEx(int numReg, int* numQubits, int precision) {
     c->dx[r] = sqrt(2.0 * PI / (double)(1 << numQubits[r]));  // context.cu:30-31
   }
   cudaGetDevice(&c->device);
+  if (cudaDeviceGetAttribute(&c->numSMs, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess ||
+      c->numSMs < 1) {
+    cudaGetLastError();
+    c->numSMs = 148;
+  }
   if (!cuda_ok(c, cudaStreamCreate(&c->stream), "cvdvCreate stream")) {
     c->numReg = 0;
     return ctx;

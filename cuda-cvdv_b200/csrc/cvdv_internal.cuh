@@ -234,6 +234,7 @@ struct Context {
   bool initialized = false;
 
   cudaStream_t stream = nullptr;
+  int numSMs = 148;  // of the context's device
   int device = 0;
 
   // twiddle table W[m] = exp(-2 pi i m / twN) for the largest register

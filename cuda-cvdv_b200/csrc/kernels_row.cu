@@ -490,10 +490,27 @@ __device__ __forceinline__ void rr_diag(C (&v)[1 << LOGE], const RowDiag& D, uin
 }
 
 // 256-thread CTAs run two per SM; 512- and 1024-thread CTAs one
+// Ask L2 to fetch [p, p + bytes) ahead of use: bulk prefetches of 16 KB, one per
+// lane of the first warp (bytes a multiple of 16 KB, at most 32 x 16 KB).
+__device__ __forceinline__ void l2_prefetch_tile(const void* p, uint32_t bytes) {
+  const uint32_t chunk = 16384;
+  const uint32_t i = threadIdx.x;
+  if (i < bytes / chunk) {
+    const char* a = static_cast<const char*>(p) + (size_t)i * chunk;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(chunk) : "memory");
+  }
+}
+
+// Tiles of one CTA per SM (more than 256 threads) run persistent: each CTA walks
+// tiles blockIdx.x, + gridDim.x, ... and asks L2 for its next tile before working
+// on the current one, so the next load finds its data on chip while this tile's
+// butterflies run.  Smaller tiles run two CTAs per SM, which already overlap one
+// CTA's loads with the other's work; they get one tile per CTA.
 template <typename C, int LOGM, int LOGR, int LOGE>
 __global__ void __launch_bounds__(1 << (LOGM - LOGE + LOGR), (LOGM - LOGE + LOGR) > 8 ? 1 : 2)
-    k_rowr(const C* __restrict__ in, C* __restrict__ out, const __grid_constant__ RowProgram P) {
+    k_rowr(const C* __restrict__ in, C* __restrict__ out, uint64_t nTiles, const __grid_constant__ RowProgram P) {
   constexpr int E = 1 << LOGE, M = 1 << LOGM, TPR = M >> LOGE, NT = TPR << LOGR, RS = M + (M >> 4);
+  constexpr uint32_t TILE_BYTES = (uint32_t)sizeof(C) << (LOGM + LOGR);
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
   double2* lo = reinterpret_cast<double2*>(sm + (RS << LOGR));  // w_M^e, e < 64
@@ -502,26 +519,32 @@ __global__ void __launch_bounds__(1 << (LOGM - LOGE + LOGR), (LOGM - LOGE + LOGR
   const int row = tid >> (LOGM - LOGE);
   const int t = tid & (TPR - 1);
   C* smrow = sm + row * RS;
-  const uint64_t rowBase = ((uint64_t)blockIdx.x << (LOGM + LOGR)) + ((uint64_t)row << LOGM);
 
   const int scM = P.logTwN - LOGM;
   for (int i = tid; i < 64 + (M >> 6); i += NT) {
     const int e = i < 64 ? i : (i - 64) << 6;
     lo[i] = __ldg(P.tw + ((size_t)e << scM));  // lo and hi are one array
   }
-  C v[E];
-#pragma unroll
-  for (int k = 0; k < E; ++k) v[k] = in[rowBase + t + k * TPR];
   __syncthreads();
-
-  for (int o = 0; o < P.nOps; ++o) {
-    const RowOp& op = P.ops[o];
-    if (op.kind == kRowDiag) rr_diag<C, LOGM, LOGE>(v, P.diag[op.diag], rowBase, t);
-    else if (op.dir > 0) rr_stages<C, 1, LOGM, 0, LOGE>(v, smrow, t, lo, hi);
-    else rr_stages<C, -1, LOGM, 0, LOGE>(v, smrow, t, lo, hi);
-  }
+  // No barrier between tiles: after a transform's last exchange (which ends in a
+  // barrier) a thread touches shared memory again only in the next tile's first
+  // exchange, and every thread has left the old tile's exchanges by then.
+  for (uint64_t tile = blockIdx.x; tile < nTiles; tile += gridDim.x) {
+    if (NT > 256 && tile + gridDim.x < nTiles)
+      l2_prefetch_tile(in + ((tile + gridDim.x) << (LOGM + LOGR)), TILE_BYTES);
+    const uint64_t rowBase = (tile << (LOGM + LOGR)) + ((uint64_t)row << LOGM);
+    C v[E];
 #pragma unroll
-  for (int k = 0; k < E; ++k) out[rowBase + t + k * TPR] = v[k];
+    for (int k = 0; k < E; ++k) v[k] = in[rowBase + t + k * TPR];
+    for (int o = 0; o < P.nOps; ++o) {
+      const RowOp& op = P.ops[o];
+      if (op.kind == kRowDiag) rr_diag<C, LOGM, LOGE>(v, P.diag[op.diag], rowBase, t);
+      else if (op.dir > 0) rr_stages<C, 1, LOGM, 0, LOGE>(v, smrow, t, lo, hi);
+      else rr_stages<C, -1, LOGM, 0, LOGE>(v, smrow, t, lo, hi);
+    }
+#pragma unroll
+    for (int k = 0; k < E; ++k) out[rowBase + t + k * TPR] = v[k];
+  }
 }
 
 // largest row k_rowr takes (one CTA: 2^13 complex128 / 2^14 complex64 points)
@@ -542,10 +565,18 @@ static cudaError_t launch_rowr_t(Context* ctx, const RowProgram& P) {
   constexpr int M = 1 << LOGM;
   const size_t smem = (size_t)(M + (M >> 4)) * (1 << LOGR) * sizeof(C) + (64 + (M >> 6)) * sizeof(double2);
   auto kern = k_rowr<C, LOGM, LOGR, LOGE>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  const uint64_t nCta = ctx->size() >> (LOGM + LOGR);
-  kern<<<(unsigned)nCta, NT, smem, ctx->stream>>>((const C*)ctx->state(), (C*)ctx->other(), P);
+  static int resident = 0;  // CTAs per SM of this instantiation, asked once
+  cudaError_t e = cudaSuccess;
+  if (!resident) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kern, NT, smem);
+    if (e != cudaSuccess || resident < 1) return e != cudaSuccess ? e : cudaErrorInvalidConfiguration;
+  }
+  const uint64_t nTiles = ctx->size() >> (LOGM + LOGR);
+  uint64_t grid = NT > 256 ? (uint64_t)ctx->numSMs * resident : nTiles;
+  if (grid > nTiles) grid = nTiles;
+  kern<<<(unsigned)grid, NT, smem, ctx->stream>>>((const C*)ctx->state(), (C*)ctx->other(), nTiles, P);
   return cudaGetLastError();
 }
 
