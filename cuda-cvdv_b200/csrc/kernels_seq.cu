@@ -58,9 +58,15 @@ template <typename C> struct SeqReal;
 template <> struct SeqReal<double2> { using t = double; };
 template <> struct SeqReal<float2> { using t = float; };
 
+// the 2x2 matrix arrives as four values (not a pointer into the kernel's
+// parameters, which would make the compiler copy them to the stack)
+struct Mat2 {
+  double2 m0, m1, m2, m3;
+};
+
 template <typename C, int NB, int B>
-__device__ __forceinline__ void seq_pair(C* v, const double2* m) {
-  const C a00 = fromd<C>(m[0]), a01 = fromd<C>(m[1]), a10 = fromd<C>(m[2]), a11 = fromd<C>(m[3]);
+__device__ __forceinline__ void seq_pair(C* v, const Mat2 m) {
+  const C a00 = fromd<C>(m.m0), a01 = fromd<C>(m.m1), a10 = fromd<C>(m.m2), a11 = fromd<C>(m.m3);
 #pragma unroll
   for (int k = 0; k < (1 << NB); ++k) {
     if (k & (1 << B)) continue;
@@ -72,9 +78,9 @@ __device__ __forceinline__ void seq_pair(C* v, const double2* m) {
 
 // real 2x2 matrix (Ry): four real-by-complex products per butterfly
 template <typename C, int NB, int B>
-__device__ __forceinline__ void seq_pair_real(C* v, const double2* m) {
+__device__ __forceinline__ void seq_pair_real(C* v, const Mat2 m) {
   using R = typename SeqReal<C>::t;
-  const R a00 = (R)m[0].x, a01 = (R)m[1].x, a10 = (R)m[2].x, a11 = (R)m[3].x;
+  const R a00 = (R)m.m0.x, a01 = (R)m.m1.x, a10 = (R)m.m2.x, a11 = (R)m.m3.x;
 #pragma unroll
   for (int k = 0; k < (1 << NB); ++k) {
     if (k & (1 << B)) continue;
@@ -122,29 +128,43 @@ template <> __device__ __forceinline__ float2 shfl_xor_c<float2>(float2 v, int m
 // 2x2 gate on a bit split across lanes: the partner amplitude (same local index)
 // lives in lane ^ lm; `hi` is this lane's value of the bit
 template <typename C, int KL>
-__device__ __forceinline__ void seq_pair_lanes(C* v, int kind, const double2* m, int lm, int hi) {
+__device__ __forceinline__ void seq_pair_lanes(C* v, int kind, const Mat2 m, int lm, int hi) {
   using R = typename SeqReal<C>::t;
+  // four amplitudes at a time: the warp barrier between groups keeps the compiler
+  // from hoisting all KL shuffles ahead (which would double the live registers)
   if (kind == kSeqPairH) {
 #pragma unroll
-    for (int k = 0; k < KL; ++k) {
-      const C o = shfl_xor_c(v[k], lm);
-      v[k] = hi ? csub(o, v[k]) : cadd(v[k], o);
+    for (int k0 = 0; k0 < KL; k0 += 4) {
+#pragma unroll
+      for (int k = k0; k < k0 + 4; ++k) {
+        const C o = shfl_xor_c(v[k], lm);
+        v[k] = hi ? csub(o, v[k]) : cadd(v[k], o);
+      }
+      __syncwarp();
     }
   } else if (kind == kSeqPairReal) {
-    const R c0 = (R)(hi ? m[2].x : m[0].x), c1 = (R)(hi ? m[3].x : m[1].x);
+    const R c0 = (R)(hi ? m.m2.x : m.m0.x), c1 = (R)(hi ? m.m3.x : m.m1.x);
 #pragma unroll
-    for (int k = 0; k < KL; ++k) {
-      const C o = shfl_xor_c(v[k], lm);
-      const C x0 = hi ? o : v[k], x1 = hi ? v[k] : o;
-      v[k] = mk(c0 * x0.x + c1 * x1.x, c0 * x0.y + c1 * x1.y);
+    for (int k0 = 0; k0 < KL; k0 += 4) {
+#pragma unroll
+      for (int k = k0; k < k0 + 4; ++k) {
+        const C o = shfl_xor_c(v[k], lm);
+        const C x0 = hi ? o : v[k], x1 = hi ? v[k] : o;
+        v[k] = mk(c0 * x0.x + c1 * x1.x, c0 * x0.y + c1 * x1.y);
+      }
+      __syncwarp();
     }
   } else {
-    const C c0 = fromd<C>(hi ? m[2] : m[0]), c1 = fromd<C>(hi ? m[3] : m[1]);
+    const C c0 = fromd<C>(hi ? m.m2 : m.m0), c1 = fromd<C>(hi ? m.m3 : m.m1);
 #pragma unroll
-    for (int k = 0; k < KL; ++k) {
-      const C o = shfl_xor_c(v[k], lm);
-      const C x0 = hi ? o : v[k], x1 = hi ? v[k] : o;
-      v[k] = cadd(cmul(c0, x0), cmul(c1, x1));
+    for (int k0 = 0; k0 < KL; k0 += 4) {
+#pragma unroll
+      for (int k = k0; k < k0 + 4; ++k) {
+        const C o = shfl_xor_c(v[k], lm);
+        const C x0 = hi ? o : v[k], x1 = hi ? v[k] : o;
+        v[k] = cadd(cmul(c0, x0), cmul(c1, x1));
+      }
+      __syncwarp();
     }
   }
 }
@@ -185,23 +205,27 @@ __global__ void __launch_bounds__(256, 2) k_seq(C* __restrict__ st, IDX nSites,
 #pragma unroll
     for (int i = 0; i < SPLIT; ++i)
       if ((part >> i) & 1) hoff += (IDX)1 << P.bits[NBL + i];
+    // the offsets are re-read from shared memory (a broadcast) at every use rather
+    // than held in KL registers across the site's gates
+    const volatile IDX* vso = soff;
     C v[KL];
 #pragma unroll
-    for (int k = 0; k < KL; ++k) v[k] = st[base + hoff + soff[k]];
+    for (int k = 0; k < KL; ++k) v[k] = st[base + hoff + vso[k]];
     R sc = (R)1;  // pending real factor of Hadamard-type pairs
     for (int o = 0; o < P.nOps; ++o) {
       const SeqOp& op = P.ops[o];
       if (op.kind != kSeqDiag) {
-        if (op.kind == kSeqPairH) sc *= (R)op.m[0].x;
+        const Mat2 mm{op.m[0], op.m[1], op.m[2], op.m[3]};
+        if (op.kind == kSeqPairH) sc *= (R)mm.m0.x;
         if (SPLIT > 0 && op.bit >= NBL) {
           const int lb = op.bit - NBL;
-          seq_pair_lanes<C, KL>(v, op.kind, op.m, 1 << lb, (part >> lb) & 1);
+          seq_pair_lanes<C, KL>(v, op.kind, mm, 1 << lb, (part >> lb) & 1);
         } else if (op.kind == kSeqPairH) {
           SEQ_BIT_SWITCH(op.bit, (seq_pair_h<C, NBL, B_>(v)))
         } else if (op.kind == kSeqPairReal) {
-          SEQ_BIT_SWITCH(op.bit, (seq_pair_real<C, NBL, B_>(v, op.m)))
+          SEQ_BIT_SWITCH(op.bit, (seq_pair_real<C, NBL, B_>(v, mm)))
         } else {
-          SEQ_BIT_SWITCH(op.bit, (seq_pair<C, NBL, B_>(v, op.m)))
+          SEQ_BIT_SWITCH(op.bit, (seq_pair<C, NBL, B_>(v, mm)))
         }
       } else {
         const SeqDiag& D = P.diag[op.diag];
@@ -234,7 +258,7 @@ __global__ void __launch_bounds__(256, 2) k_seq(C* __restrict__ st, IDX nSites,
       for (int k = 0; k < KL; ++k) v[k] = mk(v[k].x * sc, v[k].y * sc);
     }
 #pragma unroll
-    for (int k = 0; k < KL; ++k) st[base + hoff + soff[k]] = v[k];
+    for (int k = 0; k < KL; ++k) st[base + hoff + vso[k]] = v[k];
   }
 }
 
