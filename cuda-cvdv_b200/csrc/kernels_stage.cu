@@ -60,7 +60,7 @@ __device__ __forceinline__ C phase_factor(const CvdvBatchPhase& P, int j, int N,
   using R = typename StageReal<C>::t;
   R s, c;
   if constexpr (sizeof(R) == sizeof(float)) {
-    sincosf((float)ph, &s, &c);
+    __sincosf((float)ph, &s, &c);  // |ph| <= pi after the FP64 reduction
   } else {
     sincos(ph, &s, &c);
   }
@@ -100,10 +100,18 @@ __device__ __forceinline__ void stage_row_task(C* __restrict__ st, const CvdvBat
       const double zs = (P.ctrlBit >= 0 && (((rowIdx << LOGN) >> P.ctrlBit) & 1ull)) ? -1.0 : 1.0;
 #pragma unroll
       for (int k = 0; k < E; ++k) v[k] = cmul(v[k], phase_factor<C>(P, t + k * TPR, N, zs));
-    } else if (op == 1) {
+    } else if (op == 1 || op == 2) {
+      // one transform body for both directions (keeps the kernel's code small):
+      // the unnormalised inverse DFT is conj(DFT(conj(x)))
+      if (op == 2) {
+#pragma unroll
+        for (int k = 0; k < E; ++k) v[k].y = -v[k].y;
+      }
       rr_stages<C, 1, LOGN, 0, LOGE>(v, smrow, t, lo, hi);
-    } else if (op == 2) {
-      rr_stages<C, -1, LOGN, 0, LOGE>(v, smrow, t, lo, hi);
+      if (op == 2) {
+#pragma unroll
+        for (int k = 0; k < E; ++k) v[k].y = -v[k].y;
+      }
     } else {  // parity: element j <- element N-1-j of the same row
 #pragma unroll
       for (int k = 0; k < E; ++k) smrow[rpad<C>(N - 1 - (t + k * TPR))] = v[k];
