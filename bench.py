@@ -282,7 +282,7 @@ def run_gpu(args, world, rank, local):
     # scaled by the 16x larger state: the kernels stream the state once per launch,
     # so their traffic grows with the rows / sites processed.
     ncu_traffic_2p24 = {"fft_pass": ((269.3 + 219.8) + (269.1 + 222.2)) / 2 * 1e6,  # k_rowc, two launches
-                        "seq": (269.5 + 209.9) * 1e6}                                  # k_seq<double2, 2>
+                        "seq": (272.4 + 214.5) * 1e6}                                  # k_seq<double2, 5, 1>
     scale = n_amp / float(1 << 24)
     traffic = ncu_traffic_2p24[dom] * scale if (dom in ncu_traffic_2p24 and args.workload == "full") else None
     achieved = kr[dom]["achieved_gbs"]
@@ -319,7 +319,8 @@ def run_gpu(args, world, rank, local):
     ms64, stats64, launches64, clocks64, norm64 = timed_run("complex64")
     kr64 = kern_roof(stats64, alg_bytes // 2)
 
-    extras = {} if args.no_extras else {"batched_c4": batched_c4(args), "variational_c5": variational_c5(args)}
+    extras = {} if args.no_extras else {"gaussian_network_c3": gaussian_c3(args), "batched_c4": batched_c4(args),
+                                         "variational_c5": variational_c5(args)}
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -404,6 +405,43 @@ def batched_c4(args):
                                   "how": "CudaCvdv complex64, one instance after another, wall clock"},
             "speedup_vs_loop": (len(insts) / (ms * 1e-3)) / (loop_n / loop_s),
             "note": "whole batch is L2-resident (state_bytes < 126 MB)"}
+
+
+def gaussian_c3(args):
+    """Two modes [13, 13] (2^26 amplitudes), complex128 and complex64: layers of (beam splitter,
+    rotation of each mode, displacement of each mode); 20 layers per step, then the Wigner
+    function of mode 0 (8192 x 8192, read back)."""
+    import torch
+    from cvdv_b200 import CudaCvdv, _lib
+    from cvdv_b200 import workloads as W
+    L = _lib.load()
+    layers = 20
+    circ = W.gaussian_network(layers=layers)
+    out = {"unit": "layers/s", "layers_per_step": layers, "gates_per_layer": len(circ["gates"]) // layers}
+    for prec in ("complex128", "complex64"):
+        sim = CudaCvdv(circ["qubits"], precision=prec, check_errors=True)
+        sim.initStateVector(W.separable_arrays(circ, device="cuda"))
+        W.apply(sim, circ["prep"])
+        W.apply(sim, circ["gates"])  # warm-up
+        sim.synchronize()
+        stream = torch.cuda.ExternalStream(L.cvdvGetStream(sim.ctx))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = max(1, min(args.steps, 3))
+        e0.record(stream)
+        for _ in range(reps):
+            W.apply(sim, circ["gates"])
+            L.cvdvFlush(sim.ctx)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / (reps * layers)
+        t0 = time.perf_counter()
+        w = sim.getWigner(0)
+        wig_s = time.perf_counter() - t0
+        out[prec] = {"value": 1e3 / ms, "ms_per_layer": ms, "wigner_s": wig_s, "wigner_shape": list(w.shape)}
+        del sim
+        torch.cuda.empty_cache()
+    out["value"] = out["complex128"]["value"]
+    return out
 
 
 def variational_c5(args):
