@@ -496,6 +496,7 @@ void cvdvSetFusion(CVDVContext* ctx, int flags) {
   if (!ctx) return;
   C(ctx)->cancelFt = (flags & 1) != 0;
   C(ctx)->fuseSeq = (flags & 2) != 0;
+  C(ctx)->colFft = (flags & 4) != 0;
 }
 
 long long cvdvCancelledTransforms(CVDVContext* ctx) { return ctx ? C(ctx)->ftCancelled * 2 : 0; }

@@ -204,7 +204,8 @@ enum KernelKind : int {
   kKReduce = 6,
   kKPhaseSpace = 7,
   kKSeq = 8,
-  kKindCount = 9,
+  kKCol = 9,
+  kKindCount = 10,
 };
 
 struct TimingRec {
@@ -260,6 +261,7 @@ struct Context {
   // dropped from the queue.  On by default (cvdvSetFusion).
   bool cancelFt = true;
   bool fuseSeq = true;  // run chains of qubit gates as one qubit-gate sequence pass
+  bool colFft = true;   // transforms of strided registers by the register-resident column kernel
   // Inside one flush, between a forward and an inverse 2^14-point transform of
   // the last register run by the two-CTA row kernel, that register may be stored
   // "blocked": position r M + k2 holds logical index r + 2 k2 (the transform's
@@ -315,6 +317,8 @@ bool launch_pair(Context* ctx, int bit, const double2 m[4], const FactorList& pr
                  const FactorList& post);
 bool launch_perm(Context* ctx, const Stage& st, const FactorList& pre, const FactorList& post);
 bool launch_fft(Context* ctx, int reg, int dir, const FactorList& pre, const FactorList& post);
+bool col_fft_ok(Context* ctx, int reg);
+bool launch_col_fft(Context* ctx, int reg, int dir, const FactorList& pre, const FactorList& post);
 bool launch_fft_generic(Context* ctx, const void* in, void* out, void* tmp, uint64_t O,
                         int q, uint64_t S, int dir, int prec);
 bool launch_init_product(Context* ctx, const double2* const* regArrays);

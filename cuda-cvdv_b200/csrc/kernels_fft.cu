@@ -337,6 +337,7 @@ static bool run_passes(Context* ctx, const void* src, void* const* dsts, uint64_
 
 // FFT along register `reg` of the live state (ping-pong buffers).
 bool launch_fft(Context* ctx, int reg, int dir, const FactorList& pre, const FactorList& post) {
+  if (ctx->colFft && col_fft_ok(ctx, reg)) return launch_col_fft(ctx, reg, dir, pre, post);
   int q = ctx->q[reg];
   int logS = ctx->flw[reg];
   uint64_t O = 1ull << (ctx->totalQbt - q - logS);

@@ -55,9 +55,10 @@ class CudaCvdv:
     def setFusion(self, on) -> None:
         """(addition) queue optimisations, all on by default: bit 0 cancels
         FtP2Q/FtQ2P pairs separated only by gates on other registers (exact
-        identity); bit 1 runs chains of qubit gates on up to four qubits as one
-        pass.  True = both, False = neither, an int = those bits."""
-        flags = (3 if on else 0) if isinstance(on, bool) else int(on)
+        identity); bit 1 runs chains of qubit gates on up to five qubits as one
+        pass; bit 2 transforms non-last registers with the register-resident
+        column kernel.  True = all, False = none, an int = those bits."""
+        flags = (7 if on else 0) if isinstance(on, bool) else int(on)
         self._L.cvdvSetFusion(self.ctx, flags)
 
     def __del__(self):

@@ -158,8 +158,11 @@ void* cvdvGetStream(CVDVContext* ctx);
  * FtQ2P(r) (or the reverse) with only stages that leave register r untouched in
  * between is removed from the queue -- the pair is the identity, so the result
  * is unchanged up to rounding.  flags bit 1 (default on): consecutive 2x2 qubit
- * gates on up to four distinct qubits, with the diagonal runs between them, run
- * as one pass over the state instead of one pass per gate.  cvdvCancelledTransforms
+ * gates on up to five distinct qubits, with the diagonal runs between them, run
+ * as one pass over the state instead of one pass per gate.  flags bit 2 (default
+ * on): transforms of a register that is not the last one run as register-resident
+ * column DFTs (one pass up to 2^8 points, two passes up to 2^16) instead of the
+ * shared-memory tile passes.  cvdvCancelledTransforms
  * counts the transforms removed so far. */
 void cvdvSetFusion(CVDVContext* ctx, int flags);
 long long cvdvCancelledTransforms(CVDVContext* ctx);
@@ -169,7 +172,8 @@ unsigned long long cvdvLaunchCount(void);
  * event pair.  cvdvGetKernelStats waits for the stream, returns the number of
  * kernel kinds, fills total milliseconds and launch counts per kind
  * (0 FFT pass, 1 qubit pair, 2 diagonal run, 3 permutation, 4 factor table,
- * 5 initialiser, 6 reduction, 7 phase space, 8 qubit-gate sequence) and resets
+ * 5 initialiser, 6 reduction, 7 phase space, 8 qubit-gate sequence, 9 column
+ * transform pass) and resets
  * them. */
 void cvdvSetTiming(CVDVContext* ctx, int on);
 int cvdvGetKernelStats(CVDVContext* ctx, double* msOut, long long* countOut, int n);

@@ -161,7 +161,9 @@ def test_fidelities():
 
 
 @pytest.mark.parametrize("qubits,reg", [([13, 3], 0), ([3, 13], 1), ([12, 2], 0), ([2, 12], 1),
-                                        ([14, 1], 0), ([1, 14], 1), ([5, 11, 2], 1), ([4, 4, 4, 4], 2)])
+                                        ([14, 1], 0), ([1, 14], 1), ([5, 11, 2], 1), ([4, 4, 4, 4], 2),
+                                        ([4, 4, 4, 4], 1), ([8, 6], 0), ([5, 7, 3], 0), ([6, 9, 3], 1),
+                                        ([10, 4], 0), ([16, 3], 0), ([2, 13, 5], 1)])
 def test_fft_layouts(qubits, reg):
     """Single- and two-pass transforms on contiguous, inner and outer registers."""
     rng = np.random.default_rng(sum(qubits) * 7 + reg)
@@ -194,6 +196,36 @@ def test_fft_layouts(qubits, reg):
         o.phase_x2(reg, -0.2)
         o.ft_q2p(reg)
         assert rel(sim.getState(), o.get_state()) < tol
+
+
+@pytest.mark.parametrize("qubits,reg", [([8, 6], 0), ([10, 4], 0), ([16, 3], 0), ([2, 13, 5], 1)])
+def test_column_transform_matches_tile_passes(qubits, reg):
+    """The register-resident column kernel against the shared-memory tile passes
+    (fusion bit 2 off) on a strided register, with diagonal runs on both sides."""
+    from cvdv_b200 import _lib
+    rng = np.random.default_rng(sum(qubits) * 5 + reg)
+    n = sum(qubits)
+    psi = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    psi /= np.linalg.norm(psi)
+    o = oracle(qubits, psi)
+    o.phase_x2(reg, 0.07)
+    o.ft_q2p(reg)
+    o.displacement(reg, 0.4, 0.1)
+    ref = o.get_state()
+    for prec, tol in (("complex128", PLAIN_TOL), ("complex64", MIXED_TOL)):
+        outs = {}
+        for flags in (7, 3):
+            sim = make(qubits, psi, prec)
+            sim.setFusion(flags)
+            _lib.load().cvdvSetTiming(sim.ctx, 1)
+            sim.sheer(reg, 0.07)
+            sim.ftQ2P(reg)
+            sim.d(reg, 0.4 + 0.1j)
+            outs[flags] = sim.getState()
+            stats = _lib.kernel_stats(sim.ctx)
+            assert (stats["col"][1] > 0) == (flags == 7), (prec, flags, stats)
+            assert rel(outs[flags], ref) < tol, (prec, flags)
+        assert rel(outs[7], outs[3]) < tol
 
 
 @pytest.mark.parametrize("n_qubits,mode_qubits", [(3, 10), (4, 13), (2, 14)])
