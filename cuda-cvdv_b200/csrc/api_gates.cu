@@ -497,6 +497,7 @@ void cvdvSetFusion(CVDVContext* ctx, int flags) {
   C(ctx)->cancelFt = (flags & 1) != 0;
   C(ctx)->fuseSeq = (flags & 2) != 0;
   C(ctx)->colFft = (flags & 4) != 0;
+  C(ctx)->colProg = (flags & 8) != 0;
 }
 
 long long cvdvCancelledTransforms(CVDVContext* ctx) { return ctx ? C(ctx)->ftCancelled * 2 : 0; }

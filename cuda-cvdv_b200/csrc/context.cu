@@ -349,6 +349,14 @@ static bool diag_fits(Context* ctx, const std::vector<Term>& terms) {
   return tables <= kMaxTab && nxx <= kMaxXX;
 }
 
+// Whether a diagonal run fits a program on register reg: the row kernels' split
+// (row programs, and column programs on k_rowr), else one factor list (column
+// transform runs).
+static bool program_diag_fits(Context* ctx, int reg, const std::vector<Term>& terms) {
+  if (ctx->flw[reg] == 0 || col_program_ok(ctx, reg)) return row_diag_fits(ctx, reg, terms);
+  return diag_fits(ctx, terms);
+}
+
 struct Op {
   const Stage* st = nullptr;        // pass-kernel op (FFT pass / pair / permutation)
   std::vector<Term> pre, post;
@@ -490,7 +498,8 @@ bool flush(Context* ctx) {
       ++i;
       continue;
     }
-    if (s.kind == kStFft && row_eligible(ctx, s.reg)) {
+    const bool chain = s.kind == kStFft && ctx->colFft && col_fft_ok(ctx, s.reg);
+    if (s.kind == kStFft && (row_eligible(ctx, s.reg) || col_program_ok(ctx, s.reg) || chain)) {
       // a row program: every following FFT on this register and every diagonal
       // run between / after them, in order, up to the program limits
       Op op;
@@ -500,12 +509,12 @@ bool flush(Context* ctx) {
         if (!op.row.empty() && op.row.back().kind == kRowDiag) {
           std::vector<Term> merged = op.row.back().terms;
           merged.insert(merged.end(), t.begin(), t.end());
-          if (!row_diag_fits(ctx, s.reg, merged)) return false;
+          if (!program_diag_fits(ctx, s.reg, merged)) return false;
           op.row.back().terms = std::move(merged);
           return true;
         }
         if (nDiag >= kMaxRowDiags || (int)op.row.size() >= kMaxRowOps ||
-            !row_diag_fits(ctx, s.reg, t))
+            !program_diag_fits(ctx, s.reg, t))
           return false;
         op.row.push_back({kRowDiag, 0, t});
         ++nDiag;

@@ -262,6 +262,7 @@ struct Context {
   bool cancelFt = true;
   bool fuseSeq = true;  // run chains of qubit gates as one qubit-gate sequence pass
   bool colFft = true;   // transforms of strided registers by the register-resident column kernel
+  bool colProg = true;  // programs on strided registers by the register-resident row kernel in column form
   // Inside one flush, between a forward and an inverse 2^14-point transform of
   // the last register run by the two-CTA row kernel, that register may be stored
   // "blocked": position r M + k2 holds logical index r + 2 k2 (the transform's
@@ -318,6 +319,7 @@ bool launch_pair(Context* ctx, int bit, const double2 m[4], const FactorList& pr
 bool launch_perm(Context* ctx, const Stage& st, const FactorList& pre, const FactorList& post);
 bool launch_fft(Context* ctx, int reg, int dir, const FactorList& pre, const FactorList& post);
 bool col_fft_ok(Context* ctx, int reg);
+bool col_program_ok(Context* ctx, int reg);
 bool launch_col_fft(Context* ctx, int reg, int dir, const FactorList& pre, const FactorList& post);
 bool launch_fft_generic(Context* ctx, const void* in, void* out, void* tmp, uint64_t O,
                         int q, uint64_t S, int dir, int prec);
@@ -334,6 +336,8 @@ struct HostRowOp {
 };
 bool row_eligible(Context* ctx, int reg);
 bool row_diag_fits(Context* ctx, int reg, const std::vector<Term>& terms);
+// a run of transforms and diagonal runs on a strided register (kernels_col.cu)
+bool launch_col_chain(Context* ctx, int reg, const std::vector<HostRowOp>& ops);
 // blockedIn: the register is stored blocked and the program starts with an
 // inverse transform; blockedOut: leave it blocked after the final forward transform
 bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops, bool blockedIn = false,

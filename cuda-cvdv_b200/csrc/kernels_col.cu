@@ -1,5 +1,5 @@
 // Transforms along a strided register (any register but the last): register-
-// resident column DFTs, one or two HBM passes.
+// resident column DFTs in coalesced passes, with runs of transforms chained.
 //
 // The state is an [O][N][S] array around register r (N = 2^q points, S = 2^f
 // amplitudes below it).  A "column" is one transform line: fixed outer and inner
@@ -7,14 +7,21 @@
 // columns (adjacent inner indices, so every load and store instruction covers W
 // consecutive amplitudes) and keeps each column's L points in registers, 16 per
 // thread; the Stockham stages of the row kernels (row_fft.cuh) exchange through
-// one padded shared-memory line per column.
+// one padded shared-memory line per column.  A pass runs a small program on its
+// columns: DFTs, diagonal runs (factor lists of the flat index) and the four-step
+// twiddle.
 //
-// Registers of up to 2^8 points take one pass.  Longer ones use the four-step
-// split N = N1 N2, j = j1 + N1 j2, k = k2 + N2 k1:
+// Registers of up to 2^8 points hold the whole column: a run of transforms and
+// diagonal gates is one pass.  Longer ones use the four-step split N = N1 N2,
+// j = j1 + N1 j2, k = k2 + N2 k1:
 //   pass 1: u[j1, k2] = w_N^{j1 k2} sum_j2 w_N2^{j2 k2} x[j1 + N1 j2]   (stored at j1 + N1 k2)
 //   pass 2: X[k2 + N2 k1] = sum_j1 w_N1^{j1 k1} u[j1, k2]            (stored in natural order)
-// The diagonal run before the transform is applied on pass 1's loads and the
-// one after it on the last pass's stores, as factors of the flat index.
+// For fixed k2, pass 2 of one transform writes the positions k2 + N2 k1, and
+// pass 1 of a next transform split the other way round (N1' = N2, N2' = N1) reads,
+// for fixed j1' = k2, exactly the positions j1' + N1' j2'.  So consecutive
+// transforms alternate their split and share a pass: pass 2 of transform t, the
+// diagonal run between, and pass 1 of transform t + 1 run on one column load --
+// T transforms take T + 1 passes instead of 2T.
 
 #include "cvdv_internal.cuh"
 #include "row_fft.cuh"
@@ -22,6 +29,16 @@
 namespace cvdv {
 
 constexpr int kColThreads = 256;
+constexpr int kMaxColOps = 24;
+constexpr int kMaxColDiags = 10;
+
+enum ColOpKind : int { kColDft = 0, kColDiag = 1 };
+
+struct ColOp {
+  int kind;
+  int dir;   // DFT: +1 forward, -1 inverse
+  int diag;  // diagonal run: index into ColPass::diag
+};
 
 struct ColPass {
   uint64_t nCols;
@@ -29,11 +46,12 @@ struct ColPass {
   int logA;           // log2 of the middle index range of a column's base
   uint64_t midIn, outerIn, axisIn;     // strides (amplitudes) of the input
   uint64_t midOut, outerOut, axisOut;  // strides of the output
-  int logN;           // > 0: multiply output point m of column (mid) by w_N^{mid m}
+  int logN;           // four-step twiddle: multiply point m of column (mid) by w_N^{mid m}
   int logTwN;
   const double2* tw;  // w_{2^logTwN}^e table of the context
-  int hasPre, hasPost;
-  FactorList pre, post;
+  int nOps, nDiag;
+  ColOp ops[kMaxColOps];
+  FactorList diag[kMaxColDiags];  // evaluated at input addresses before the first DFT, output ones after
 };
 
 template <int LOGL>
@@ -43,11 +61,26 @@ struct ColShape {
   static constexpr int HI = L >= 64 ? (L >> 6) : 1;
 };
 
-template <typename C, int LOGL, int DIR>
+// Pass shapes: the first half of a transform (diagonal runs on the loads, DFT,
+// four-step twiddle), a shared middle pass (DFT, runs, DFT, twiddle), the second
+// half (DFT, runs on the stores), or a whole run on a short register (the op list).
+enum ColKind : int { kColFirst = 0, kColMiddle = 1, kColLast = 2, kColWhole = 3 };
+
+template <typename C, int LOGL>
+__device__ __forceinline__ void col_diags(C (&v)[16], const ColPass& P, uint64_t b, uint64_t ax, int t) {
+  constexpr int TPC = ColShape<LOGL>::TPC;
+  for (int d = 0; d < P.nDiag; ++d) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k)
+      v[k] = cmul(v[k], fromd<C>(eval_factor(P.diag[d], b + (uint64_t)(t + TPC * k) * ax)));
+  }
+}
+
+template <typename C, int LOGL, int KIND, int D1, int D2>
 __global__ void __launch_bounds__(kColThreads, 2)
     k_colr(const C* __restrict__ in, C* __restrict__ out, const __grid_constant__ ColPass P) {
   using S = ColShape<LOGL>;
-  constexpr int L = S::L, TPC = S::TPC, W = S::W;
+  constexpr int TPC = S::TPC, W = S::W;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
   double2* loL = reinterpret_cast<double2*>(sm + (size_t)W * S::RS);  // w_L^e, e < 64
@@ -81,137 +114,221 @@ __global__ void __launch_bounds__(kColThreads, 2)
   const uint64_t o = c >> (P.logS + P.logA);
   const uint64_t bIn = i + mid * P.midIn + o * P.outerIn;
   const uint64_t bOut = i + mid * P.midOut + o * P.outerOut;
+  C* smcol = sm + (size_t)w * S::RS;
   C v[16];
+  // the first half's diagonal runs ride on the loads, the last half's on the stores
 #pragma unroll
   for (int k = 0; k < 16; ++k) {
     const uint64_t a = bIn + (uint64_t)(t + TPC * k) * P.axisIn;
     v[k] = in[a];
-    if (P.hasPre) v[k] = cmul(v[k], fromd<C>(eval_factor(P.pre, a)));
+    if constexpr (KIND == kColFirst)
+      for (int d = 0; d < P.nDiag; ++d) v[k] = cmul(v[k], fromd<C>(eval_factor(P.diag[d], a)));
   }
-  rr_stages<C, DIR, LOGL, 0, 4>(v, sm + (size_t)w * S::RS, t, loL, hiL);
+  if constexpr (KIND == kColWhole) {
+    // input and output addresses coincide (one pass over the whole register)
+    for (int p = 0; p < P.nOps; ++p) {
+      const ColOp& op = P.ops[p];
+      if (op.kind == kColDft) {
+        if (op.dir > 0) rr_stages<C, 1, LOGL, 0, 4>(v, smcol, t, loL, hiL);
+        else rr_stages<C, -1, LOGL, 0, 4>(v, smcol, t, loL, hiL);
+      } else {
+        const FactorList& F = P.diag[op.diag];
+#pragma unroll
+        for (int k = 0; k < 16; ++k)
+          v[k] = cmul(v[k], fromd<C>(eval_factor(F, bOut + (uint64_t)(t + TPC * k) * P.axisOut)));
+      }
+    }
+  } else {
+    rr_stages<C, D1, LOGL, 0, 4>(v, smcol, t, loL, hiL);
+    if constexpr (KIND == kColMiddle) {
+      col_diags<C, LOGL>(v, P, bOut, P.axisOut, t);
+      rr_stages<C, D2, LOGL, 0, 4>(v, smcol, t, loL, hiL);
+    }
+  }
+  constexpr int DT = KIND == kColMiddle ? D2 : D1;  // direction of the four-step twiddle
   const int nMask = (1 << P.logN) - 1;
 #pragma unroll
   for (int k = 0; k < 16; ++k) {
     const int m = t + TPC * k;
     const uint64_t a = bOut + (uint64_t)m * P.axisOut;
     C x = v[k];
-    if (P.logN > 0) {
+    if constexpr (KIND == kColFirst || KIND == kColMiddle) {
       const int e = (int)((mid * (uint64_t)m) & (uint64_t)nMask);
-      if (e) x = cmul(x, tw2<C, DIR>(loN, hiN, e));
+      if (e) x = cmul(x, tw2<C, DT>(loN, hiN, e));
     }
-    if (P.hasPost) x = cmul(x, fromd<C>(eval_factor(P.post, a)));
+    if constexpr (KIND == kColLast)
+      for (int d = 0; d < P.nDiag; ++d) x = cmul(x, fromd<C>(eval_factor(P.diag[d], a)));
     out[a] = x;
   }
 }
 
-template <typename C, int LOGL>
-static cudaError_t col_launch(Context* ctx, const void* in, void* out, const ColPass& P, int dir) {
+template <typename C, int LOGL, int KIND, int D1, int D2>
+static cudaError_t col_launch_t(Context* ctx, const ColPass& P) {
   using S = ColShape<LOGL>;
   const int nHiN = P.logN >= 6 ? 1 << (P.logN - 6) : 1;
   const size_t smem = (size_t)S::W * S::RS * sizeof(C) + (64 + S::HI + 64 + nHiN) * sizeof(double2);
   const unsigned grid = (unsigned)(P.nCols / S::W);
-  cudaError_t e;
-  if (dir > 0) {
-    e = cudaFuncSetAttribute(k_colr<C, LOGL, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess) k_colr<C, LOGL, 1><<<grid, kColThreads, smem, ctx->stream>>>((const C*)in, (C*)out, P);
-  } else {
-    e = cudaFuncSetAttribute(k_colr<C, LOGL, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess) k_colr<C, LOGL, -1><<<grid, kColThreads, smem, ctx->stream>>>((const C*)in, (C*)out, P);
+  auto kern = k_colr<C, LOGL, KIND, D1, D2>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  kern<<<grid, kColThreads, smem, ctx->stream>>>((const C*)ctx->state(), (C*)ctx->other(), P);
+  return cudaGetLastError();
+}
+
+template <typename C, int LOGL>
+static cudaError_t col_launch(Context* ctx, const ColPass& P, int kind, int d1, int d2) {
+  switch (kind) {
+    case kColFirst:
+      return d1 > 0 ? col_launch_t<C, LOGL, kColFirst, 1, 0>(ctx, P) : col_launch_t<C, LOGL, kColFirst, -1, 0>(ctx, P);
+    case kColLast:
+      return d1 > 0 ? col_launch_t<C, LOGL, kColLast, 1, 0>(ctx, P) : col_launch_t<C, LOGL, kColLast, -1, 0>(ctx, P);
+    case kColMiddle:
+      if (d1 > 0) return d2 > 0 ? col_launch_t<C, LOGL, kColMiddle, 1, 1>(ctx, P) : col_launch_t<C, LOGL, kColMiddle, 1, -1>(ctx, P);
+      return d2 > 0 ? col_launch_t<C, LOGL, kColMiddle, -1, 1>(ctx, P) : col_launch_t<C, LOGL, kColMiddle, -1, -1>(ctx, P);
+    default:
+      return col_launch_t<C, LOGL, kColWhole, 1, 0>(ctx, P);
   }
-  return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 template <typename C>
-static cudaError_t col_dispatch(Context* ctx, int logL, const void* in, void* out, const ColPass& P, int dir) {
+static cudaError_t col_dispatch(Context* ctx, int logL, const ColPass& P, int kind, int d1, int d2) {
   switch (logL) {
-    case 4: return col_launch<C, 4>(ctx, in, out, P, dir);
-    case 5: return col_launch<C, 5>(ctx, in, out, P, dir);
-    case 6: return col_launch<C, 6>(ctx, in, out, P, dir);
-    case 7: return col_launch<C, 7>(ctx, in, out, P, dir);
-    default: return col_launch<C, 8>(ctx, in, out, P, dir);
+    case 4: return col_launch<C, 4>(ctx, P, kind, d1, d2);
+    case 5: return col_launch<C, 5>(ctx, P, kind, d1, d2);
+    case 6: return col_launch<C, 6>(ctx, P, kind, d1, d2);
+    case 7: return col_launch<C, 7>(ctx, P, kind, d1, d2);
+    default: return col_launch<C, 8>(ctx, P, kind, d1, d2);
   }
 }
 
-// Whether launch_col_fft takes a transform of register `reg`: 2^4..2^16 points and
-// at least 8 amplitudes below it (runs of 8 contiguous columns for the loads and
-// stores).  A pass of 2^l points has 2^(n-l) columns and 2^(12-l) columns per
+// Whether the column kernel takes transforms of register `reg`: 2^4..2^16 points
+// and at least 8 amplitudes below it (runs of 8 contiguous columns for the loads
+// and stores).  A pass of 2^l points has 2^(n-l) columns and 2^(12-l) columns per
 // CTA, so n >= 12 fills every CTA.
 bool col_fft_ok(Context* ctx, int reg) {
   const int q = ctx->q[reg], logS = ctx->flw[reg];
   return q >= 4 && q <= 16 && logS >= 3 && ctx->totalQbt >= 12;
 }
 
-bool launch_col_fft(Context* ctx, int reg, int dir, const FactorList& pre, const FactorList& post) {
+// A run of T >= 1 transforms (directions dirs) with the diagonal runs around
+// them: slots[0] before the first, slots[t] between transform t-1 and t,
+// slots[T] after the last (each slot a list of diagonal runs).
+static bool run_col_chain(Context* ctx, int reg, const std::vector<int>& dirs,
+                          const std::vector<std::vector<FactorList>>& slots) {
   const int q = ctx->q[reg], logS = ctx->flw[reg], n = ctx->totalQbt;
+  const int T = (int)dirs.size();
   const uint64_t S = 1ull << logS, N = 1ull << q;
   int logTwN = 0;
   while ((1 << logTwN) < ctx->twN) ++logTwN;
-  ColPass P{};
-  P.logS = logS;
-  P.logTwN = logTwN;
-  P.tw = ctx->twiddle;
-  const bool two = q > 8;
-  const int a = two ? (q + 1) / 2 : q, b = q - a;  // N1 = 2^a, N2 = 2^b
-  cudaError_t e;
-  const void* src = ctx->state();
-  void* dst = ctx->other();
-  {
-    LaunchScope _ls(ctx, kKCol);
-    if (!two) {
-      P.nCols = 1ull << (n - q);
-      P.logA = 0;
-      P.midIn = P.midOut = 0;
-      P.outerIn = P.outerOut = N * S;
-      P.axisIn = P.axisOut = S;
-      P.logN = 0;
-      P.hasPre = !factor_empty(pre);
-      P.hasPost = !factor_empty(post);
-      P.pre = pre;
-      P.post = post;
-      e = ctx->precision == kC128 ? col_dispatch<double2>(ctx, q, src, dst, P, dir)
-                                  : col_dispatch<float2>(ctx, q, src, dst, P, dir);
-    } else {
-      // pass 1: N2-point DFTs along j2 (stride N1 S), columns (i, j1, o); twiddle w_N^{j1 k2}
-      P.nCols = 1ull << (n - b);
-      P.logA = a;
-      P.midIn = P.midOut = S;
-      P.outerIn = P.outerOut = N * S;
-      P.axisIn = P.axisOut = (1ull << a) * S;
-      P.logN = q;
-      P.hasPre = !factor_empty(pre);
-      P.pre = pre;
-      P.hasPost = 0;
-      e = ctx->precision == kC128 ? col_dispatch<double2>(ctx, b, src, dst, P, dir)
-                                  : col_dispatch<float2>(ctx, b, src, dst, P, dir);
+  auto base = [&](ColPass& P) {
+    P = ColPass{};
+    P.logS = logS;
+    P.logTwN = logTwN;
+    P.tw = ctx->twiddle;
+    P.outerIn = P.outerOut = N * S;
+  };
+  auto add_op = [&](ColPass& P, int kind, int dir, const FactorList* F) -> bool {
+    if (P.nOps >= kMaxColOps || (kind == kColDiag && P.nDiag >= kMaxColDiags)) return false;
+    ColOp& op = P.ops[P.nOps++];
+    op.kind = kind;
+    op.dir = dir;
+    op.diag = -1;
+    if (kind == kColDiag) {
+      P.diag[P.nDiag] = *F;
+      op.diag = P.nDiag++;
     }
+    return true;
+  };
+  auto add_slot = [&](ColPass& P, int s) -> bool {
+    for (const FactorList& F : slots[s])
+      if (!factor_empty(F) && !add_op(P, kColDiag, 0, &F)) return false;
+    return true;
+  };
+  auto go = [&](const ColPass& P, int logL, int kind, int d1, int d2) -> bool {
+    cudaError_t e;
+    {
+      LaunchScope _ls(ctx, kKCol);
+      e = ctx->precision == kC128 ? col_dispatch<double2>(ctx, logL, P, kind, d1, d2)
+                                  : col_dispatch<float2>(ctx, logL, P, kind, d1, d2);
+    }
+    if (!cuda_ok(ctx, e, "column transform launch")) return false;
+    ctx->cur ^= 1;
+    return true;
+  };
+  auto too_long = [&]() {
+    set_error(ctx, kErrUnsupported, "column transform run too long");
+    return false;
+  };
+  ColPass P;
+  if (q <= 8) {  // the whole run in one pass
+    base(P);
+    P.nCols = 1ull << (n - q);
+    P.axisIn = P.axisOut = S;
+    for (int t = 0; t <= T; ++t) {
+      if (!add_slot(P, t)) return too_long();
+      if (t < T && !add_op(P, kColDft, dirs[t], nullptr)) return too_long();
+    }
+    return go(P, q, kColWhole, 0, 0);
   }
-  if (!cuda_ok(ctx, e, "column transform launch")) return false;
-  ctx->cur ^= 1;
-  if (!two) return true;
-  {
-    // pass 2: N1-point DFTs along j1 (stride S), columns (i, k2, o); output k2 + N2 k1
-    LaunchScope _ls(ctx, kKCol);
-    ColPass Q{};
-    Q.logS = logS;
-    Q.logTwN = logTwN;
-    Q.tw = ctx->twiddle;
-    Q.nCols = 1ull << (n - a);
-    Q.logA = b;
-    Q.midIn = (1ull << a) * S;
-    Q.midOut = S;
-    Q.outerIn = Q.outerOut = N * S;
-    Q.axisIn = S;
-    Q.axisOut = (1ull << b) * S;
-    Q.logN = 0;
-    Q.hasPre = 0;
-    Q.hasPost = !factor_empty(post);
-    Q.post = post;
-    e = ctx->precision == kC128 ? col_dispatch<double2>(ctx, a, ctx->state(), ctx->other(), Q, dir)
-                                : col_dispatch<float2>(ctx, a, ctx->state(), ctx->other(), Q, dir);
+  const int a = (q + 1) / 2, b = q - a;
+  auto n1 = [&](int t) { return (t & 1) ? b : a; };  // log N1 of transform t
+  auto n2 = [&](int t) { return (t & 1) ? a : b; };
+  // pass 0: transform 0's N2-point DFTs along j2 (stride N1 S), columns (i, j1, o)
+  base(P);
+  P.nCols = 1ull << (n - n2(0));
+  P.logA = n1(0);
+  P.midIn = P.midOut = S;
+  P.axisIn = P.axisOut = (1ull << n1(0)) * S;
+  P.logN = q;
+  if (!add_slot(P, 0)) return too_long();
+  if (!go(P, n2(0), kColFirst, dirs[0], 0)) return false;
+  // pass t: transform t-1's N1-point DFTs along j1 (stride S), columns (i, k2, o),
+  // then (t < T) the run between and transform t's first half on the same points
+  for (int t = 1; t <= T; ++t) {
+    base(P);
+    P.nCols = 1ull << (n - n1(t - 1));
+    P.logA = n2(t - 1);
+    P.midIn = (1ull << n1(t - 1)) * S;
+    P.axisIn = S;
+    P.midOut = S;
+    P.axisOut = (1ull << n2(t - 1)) * S;
+    P.logN = t < T ? q : 0;
+    if (!add_slot(P, t)) return too_long();
+    if (!go(P, n1(t - 1), t < T ? kColMiddle : kColLast, dirs[t - 1], t < T ? dirs[t] : 0)) return false;
   }
-  if (!cuda_ok(ctx, e, "column transform launch")) return false;
-  ctx->cur ^= 1;
   return true;
+}
+
+bool launch_col_fft(Context* ctx, int reg, int dir, const FactorList& pre, const FactorList& post) {
+  return run_col_chain(ctx, reg, {dir}, {{pre}, {post}});
+}
+
+// A row-program style run (transforms of `reg` and diagonal runs, in order) on a
+// strided register: one pass for registers of up to 2^8 points, T + 1 chained
+// passes for longer ones.
+bool launch_col_chain(Context* ctx, int reg, const std::vector<HostRowOp>& ops) {
+  std::vector<int> dirs;
+  std::vector<std::vector<FactorList>> slots(1);
+  for (const HostRowOp& h : ops) {
+    if (h.kind == kRowFft) {
+      dirs.push_back(h.dir);
+      slots.emplace_back();
+      continue;
+    }
+    FactorList F;
+    std::vector<Term> left;
+    if (!build_factor_list(ctx, h.terms, &F, &left)) return false;
+    if (!left.empty()) {
+      set_error(ctx, kErrUnsupported, "column transform run: diagonal run does not fit");
+      return false;
+    }
+    slots.back().push_back(F);
+  }
+  if (dirs.empty()) {
+    set_error(ctx, kErrUnsupported, "column transform run without a transform");
+    return false;
+  }
+  return run_col_chain(ctx, reg, dirs, slots);
 }
 
 }  // namespace cvdv

@@ -70,6 +70,14 @@ struct RowDiag {
   int hasRowF, hasElemF;
   FactorList rowF;     // factors constant along a row
   FactorList elemF;    // per-element factors (bilinear terms with the row register)
+  // Bilinear terms c x_row x_other (other register and control bit off the row)
+  // taken out of elemF for k_rowr: along one row they are the linear phase
+  // a (m - regC) regDx with a = sum c x_other (+-1 by the control bit), so a
+  // thread needs two sincos per run instead of one per amplitude.  The other
+  // register is side 1 of each XXFactor.
+  int nLin;
+  double regC, regDx;
+  XXFactor lin[kMaxXX];
 };
 
 struct RowProgram {
@@ -83,6 +91,7 @@ struct RowProgram {
   int storeBlocked;  // two-CTA rows ending transposed: write the blocked layout
   int dualHead;      // two-CTA rows: index of a leading forward transform whose radix-2 step
                      // reads the whole row in both CTAs (no swap), or -1
+  int logS;          // k_rowr on a strided register: log2 of the amplitudes below it (0: rows)
   const double2* tw;
   RowOp ops[kMaxRowOps];
   RowDiag diag[kMaxRowDiags];
@@ -467,6 +476,23 @@ template <typename C, int LOGM, int LOGE>
 __device__ __forceinline__ void rr_diag(C (&v)[1 << LOGE], const RowDiag& D, uint64_t rowBase, int t) {
   constexpr int E = 1 << LOGE, TPR = 1 << (LOGM - LOGE);
   const double2 rs = D.hasRowF ? eval_factor(D.rowF, rowBase) : make_double2(1.0, 0.0);
+  // running factor of element t + k TPR: rs times the linear phase, advanced by st per k
+  double2 f = rs, st = make_double2(1.0, 0.0);
+  if (D.nLin) {
+    double a = 0.0;
+    for (int l = 0; l < D.nLin; ++l) {
+      const XXFactor& X = D.lin[l];
+      const int j = (int)((rowBase >> X.shift1) & (uint64_t)X.mask1);
+      double c = X.coeff * (((double)j - X.c1) * X.dx1);
+      if (X.ctrlShift >= 0 && ((rowBase >> X.ctrlShift) & 1ull)) c = -c;
+      a += c;
+    }
+    a *= D.regDx;
+    double s0, c0;
+    sincos(a * ((double)t - D.regC), &s0, &c0);
+    sincos(a * (double)TPR, &st.y, &st.x);
+    f = dmul(rs, make_double2(c0, s0));
+  }
   if (D.tab) {
     int seg = 0;
     for (int c = 0; c < D.nCtrl; ++c) seg |= (int)((rowBase >> D.ctrlShift[c]) & 1ull) << c;
@@ -478,9 +504,16 @@ __device__ __forceinline__ void rr_diag(C (&v)[1 << LOGE], const RowDiag& D, uin
       for (int k = 0; k < 8; ++k) w[k] = __ldg(tp + (k0 + k) * TPR);
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
-        if (D.hasRowF) w[k] = dmul(w[k], rs);
+        if (D.hasRowF || D.nLin) w[k] = dmul(w[k], f);
+        if (D.nLin) f = dmul(f, st);
         v[k0 + k] = cmul(v[k0 + k], fromd<C>(w[k]));
       }
+    }
+  } else if (D.nLin) {
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+      v[k] = cmul(v[k], fromd<C>(f));
+      f = dmul(f, st);
     }
   } else if (D.hasRowF) {
     const C c = fromd<C>(rs);
@@ -506,7 +539,13 @@ __device__ __forceinline__ void l2_prefetch_tile(const void* p, uint32_t bytes) 
 // on the current one, so the next load finds its data on chip while this tile's
 // butterflies run.  Smaller tiles run two CTAs per SM, which already overlap one
 // CTA's loads with the other's work; they get one tile per CTA.
-template <typename C, int LOGM, int LOGR, int LOGE>
+//
+// With COL the "rows" are the columns of a strided register (P.logS amplitudes
+// below it): column c is inner index c mod S and outer index c / S, and element m
+// sits m S amplitudes after its first.  The CTA's columns are adjacent inner
+// indices; a warp's loads hit 32 different sectors, whose other halves the
+// CTAs of the neighbouring columns, running at the same time, read from L2.
+template <typename C, int LOGM, int LOGR, int LOGE, bool COL>
 __global__ void __launch_bounds__(1 << (LOGM - LOGE + LOGR), (LOGM - LOGE + LOGR) > 8 ? 1 : 2)
     k_rowr(const C* __restrict__ in, C* __restrict__ out, uint64_t nTiles, const __grid_constant__ RowProgram P) {
   constexpr int E = 1 << LOGE, M = 1 << LOGM, TPR = M >> LOGE, NT = TPR << LOGR, RS = M + (M >> 4);
@@ -519,6 +558,7 @@ __global__ void __launch_bounds__(1 << (LOGM - LOGE + LOGR), (LOGM - LOGE + LOGR
   const int row = tid >> (LOGM - LOGE);
   const int t = tid & (TPR - 1);
   C* smrow = sm + row * RS;
+  const int logS = COL ? P.logS : 0;
 
   const int scM = P.logTwN - LOGM;
   for (int i = tid; i < 64 + (M >> 6); i += NT) {
@@ -530,12 +570,18 @@ __global__ void __launch_bounds__(1 << (LOGM - LOGE + LOGR), (LOGM - LOGE + LOGR
   // barrier) a thread touches shared memory again only in the next tile's first
   // exchange, and every thread has left the old tile's exchanges by then.
   for (uint64_t tile = blockIdx.x; tile < nTiles; tile += gridDim.x) {
-    if (NT > 256 && tile + gridDim.x < nTiles)
-      l2_prefetch_tile(in + ((tile + gridDim.x) << (LOGM + LOGR)), TILE_BYTES);
-    const uint64_t rowBase = (tile << (LOGM + LOGR)) + ((uint64_t)row << LOGM);
+    uint64_t rowBase;
+    if constexpr (COL) {
+      const uint64_t c = (tile << LOGR) + (uint64_t)row;
+      rowBase = (c & ((1ull << logS) - 1)) + ((c >> logS) << (LOGM + logS));
+    } else {
+      if (NT > 256 && tile + gridDim.x < nTiles)
+        l2_prefetch_tile(in + ((tile + gridDim.x) << (LOGM + LOGR)), TILE_BYTES);
+      rowBase = (tile << (LOGM + LOGR)) + ((uint64_t)row << LOGM);
+    }
     C v[E];
 #pragma unroll
-    for (int k = 0; k < E; ++k) v[k] = in[rowBase + t + k * TPR];
+    for (int k = 0; k < E; ++k) v[k] = in[rowBase + ((uint64_t)(t + k * TPR) << logS)];
     for (int o = 0; o < P.nOps; ++o) {
       const RowOp& op = P.ops[o];
       if (op.kind == kRowDiag) rr_diag<C, LOGM, LOGE>(v, P.diag[op.diag], rowBase, t);
@@ -543,7 +589,7 @@ __global__ void __launch_bounds__(1 << (LOGM - LOGE + LOGR), (LOGM - LOGE + LOGR
       else rr_stages<C, -1, LOGM, 0, LOGE>(v, smrow, t, lo, hi);
     }
 #pragma unroll
-    for (int k = 0; k < E; ++k) out[rowBase + t + k * TPR] = v[k];
+    for (int k = 0; k < E; ++k) out[rowBase + ((uint64_t)(t + k * TPR) << logS)] = v[k];
   }
 }
 
@@ -558,13 +604,13 @@ struct RrShape {
   static constexpr int LOGR = LOGM - LOGE < 8 ? 8 - (LOGM - LOGE) : 0;
 };
 
-template <typename C, int LOGM>
+template <typename C, int LOGM, bool COL>
 static cudaError_t launch_rowr_t(Context* ctx, const RowProgram& P) {
   constexpr int LOGE = RrShape<C, LOGM>::LOGE, LOGR = RrShape<C, LOGM>::LOGR;
   constexpr int NT = 1 << (LOGM - LOGE + LOGR);
   constexpr int M = 1 << LOGM;
   const size_t smem = (size_t)(M + (M >> 4)) * (1 << LOGR) * sizeof(C) + (64 + (M >> 6)) * sizeof(double2);
-  auto kern = k_rowr<C, LOGM, LOGR, LOGE>;
+  auto kern = k_rowr<C, LOGM, LOGR, LOGE, COL>;
   static int resident = 0;  // CTAs per SM of this instantiation, asked once
   cudaError_t e = cudaSuccess;
   if (!resident) {
@@ -580,19 +626,34 @@ static cudaError_t launch_rowr_t(Context* ctx, const RowProgram& P) {
   return cudaGetLastError();
 }
 
-template <typename C>
+template <typename C, bool COL>
 static cudaError_t launch_rowr(Context* ctx, const RowProgram& P, int q) {
   switch (q) {
-    case 8: return launch_rowr_t<C, 8>(ctx, P);
-    case 9: return launch_rowr_t<C, 9>(ctx, P);
-    case 10: return launch_rowr_t<C, 10>(ctx, P);
-    case 11: return launch_rowr_t<C, 11>(ctx, P);
-    case 12: return launch_rowr_t<C, 12>(ctx, P);
-    case 13: return launch_rowr_t<C, 13>(ctx, P);
+    case 8: return launch_rowr_t<C, 8, COL>(ctx, P);
+    case 9: return launch_rowr_t<C, 9, COL>(ctx, P);
+    case 10: return launch_rowr_t<C, 10, COL>(ctx, P);
+    case 11: return launch_rowr_t<C, 11, COL>(ctx, P);
+    case 12: return launch_rowr_t<C, 12, COL>(ctx, P);
+    case 13: return launch_rowr_t<C, 13, COL>(ctx, P);
     default:
-      if constexpr (sizeof(C) == sizeof(float2)) return launch_rowr_t<C, 14>(ctx, P);
+      if constexpr (sizeof(C) == sizeof(float2)) return launch_rowr_t<C, 14, COL>(ctx, P);
       return cudaErrorInvalidValue;
   }
+}
+
+// A program on a register that is not the last one runs on k_rowr in column
+// form for complex64 registers of 2^9 .. 2^14 points (at least as many columns as
+// one CTA takes).  The column loads are strided, but one pass replaces the two
+// per transform of the column kernel; in complex128 the column kernel measured
+// faster, and registers of up to 2^8 points run whole on it anyway.
+bool col_program_ok(Context* ctx, int reg) {
+  const int q = ctx->q[reg];
+  if (!ctx->colProg || ctx->precision != kC64 || ctx->flw[reg] == 0 || q <= 8 ||
+      q > rowr_max_log(ctx->precision))
+    return false;
+  const int logE = (ctx->precision == kC64 && q >= 13) ? 5 : 4;
+  const int logR = q - logE < 8 ? 8 - (q - logE) : 0;
+  return ctx->totalQbt - q >= logR;
 }
 
 // ---------------------------------------------------------------- two-CTA register-resident rows
@@ -933,10 +994,26 @@ static bool split_row_diag(Context* ctx, int reg, const std::vector<Term>& terms
   return fits(*rowTerms) && fits(*elemTerms);
 }
 
+// A bilinear term c x_reg x_other whose control bit (if any) lies off register
+// reg: along a row of reg it is a linear phase (RowDiag::lin).
+static bool linear_xx(Context* ctx, int reg, const Term& t) {
+  const int lo = ctx->flw[reg], hi = lo + ctx->q[reg];
+  return t.kind == kTermXX && ((t.r == reg) != (t.s == reg)) && (t.ctrlBit < 0 || t.ctrlBit < lo || t.ctrlBit >= hi);
+}
+
+static bool all_linear(Context* ctx, int reg, const std::vector<Term>& elemTerms) {
+  for (const Term& t : elemTerms)
+    if (!linear_xx(ctx, reg, t)) return false;
+  return true;
+}
+
+// Programs on a strided register run on k_rowr only, which takes no per-element
+// factor other than linear phases.
 bool row_diag_fits(Context* ctx, int reg, const std::vector<Term>& terms) {
   std::vector<Term> a, b, c;
   std::vector<int> bits;
-  return split_row_diag(ctx, reg, terms, &a, &bits, &b, &c);
+  if (!split_row_diag(ctx, reg, terms, &a, &bits, &b, &c)) return false;
+  return ctx->flw[reg] == 0 || all_linear(ctx, reg, c);
 }
 
 template <typename C, int LOGC, int LOGT>
@@ -992,11 +1069,28 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
   // use the big tile (512 threads, twice the amplitudes, one CTA per SM) and, past
   // that, a cluster of 2 or 4 big tiles.
   int q = ctx->q[reg];
+  const bool col = ctx->flw[reg] != 0;  // a strided register: k_rowr in column form, or the column kernel
+  if (col && !col_program_ok(ctx, reg)) return launch_col_chain(ctx, reg, ops);
   int logT = q <= row_log_tile(ctx->precision) ? 8 : 9;
   int lt = row_log_tile(ctx->precision) + (logT - 8);
   int logC = q > lt ? q - lt : 0;
-  const bool useC = rowc_takes(ctx, reg, ops);  // the two-CTA register-resident kernel
+  const bool useC = !col && rowc_takes(ctx, reg, ops);  // the two-CTA register-resident kernel
   if (useC) logC = 1;
+  if (col) logC = 0;
+  // k_rowr runs the program when every per-element factor is a linear phase
+  bool toRowr = logC == 0 && q <= rowr_max_log(ctx->precision);
+  for (const HostRowOp& h : ops) {
+    if (!toRowr || h.kind != kRowDiag) continue;
+    std::vector<Term> regTerms, rowTerms, elemTerms;
+    std::vector<int> bits;
+    toRowr = split_row_diag(ctx, reg, h.terms, &regTerms, &bits, &rowTerms, &elemTerms) &&
+             all_linear(ctx, reg, elemTerms);
+  }
+  if (col && !toRowr) {
+    set_error(ctx, kErrUnsupported, "column program on register %d needs per-element factors", reg);
+    return false;
+  }
+  P.logS = col ? ctx->flw[reg] : 0;
   P.logN = q;
   P.logM = q - logC;
   P.logRows = q < lt ? lt - q : 0;
@@ -1050,6 +1144,32 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
         return false;
       D.tab = tab;
     }
+    D.nLin = 0;
+    if (toRowr) {
+      const int lo = ctx->flw[reg];
+      std::vector<Term> rest;
+      for (const Term& t : elemTerms) {
+        if (!linear_xx(ctx, reg, t) || D.nLin >= kMaxXX) {
+          rest.push_back(t);
+          continue;
+        }
+        const int o = t.r == reg ? t.s : t.r;
+        XXFactor& X = D.lin[D.nLin++];
+        X.shift1 = ctx->flw[o];
+        X.mask1 = (1 << ctx->q[o]) - 1;
+        X.c1 = (double)((1 << ctx->q[o]) - 1) * 0.5;
+        X.dx1 = ctx->dx[o];
+        X.shift2 = lo;
+        X.mask2 = (1 << q) - 1;
+        X.c2 = (double)((1 << q) - 1) * 0.5;
+        X.dx2 = ctx->dx[reg];
+        X.coeff = t.coeff;
+        X.ctrlShift = t.ctrlBit;
+      }
+      elemTerms.swap(rest);
+      D.regC = (double)((1 << q) - 1) * 0.5;
+      D.regDx = ctx->dx[reg];
+    }
     std::vector<Term> left;
     if (!build_factor_list(ctx, rowTerms, &D.rowF, &left) || !left.empty()) return false;
     if (!build_factor_list(ctx, elemTerms, &D.elemF, &left) || !left.empty()) return false;
@@ -1090,11 +1210,18 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
     ctx->cur ^= 1;
     return true;
   }
-  if (logC == 0 && !elemF && q <= rowr_max_log(ctx->precision)) {
+  if (toRowr) {
+    if (elemF) {
+      set_error(ctx, kErrUnsupported, "row program: per-element factors left for k_rowr");
+      return false;
+    }
     cudaError_t er;
     {
-      LaunchScope _ls(ctx, kKFft);
-      er = ctx->precision == kC128 ? launch_rowr<double2>(ctx, P, q) : launch_rowr<float2>(ctx, P, q);
+      LaunchScope _ls(ctx, col ? kKCol : kKFft);
+      if (col)
+        er = ctx->precision == kC128 ? launch_rowr<double2, true>(ctx, P, q) : launch_rowr<float2, true>(ctx, P, q);
+      else
+        er = ctx->precision == kC128 ? launch_rowr<double2, false>(ctx, P, q) : launch_rowr<float2, false>(ctx, P, q);
     }
     if (!cuda_ok(ctx, er, "row program launch")) return false;
     ctx->cur ^= 1;

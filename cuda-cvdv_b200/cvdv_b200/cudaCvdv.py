@@ -57,8 +57,10 @@ class CudaCvdv:
         FtP2Q/FtQ2P pairs separated only by gates on other registers (exact
         identity); bit 1 runs chains of qubit gates on up to five qubits as one
         pass; bit 2 transforms non-last registers with the register-resident
-        column kernel.  True = all, False = none, an int = those bits."""
-        flags = (7 if on else 0) if isinstance(on, bool) else int(on)
+        column kernel; bit 3 runs transform/diagonal runs on a non-last register
+        as one pass with each column on chip.  True = all, False = none, an int
+        = those bits."""
+        flags = (15 if on else 0) if isinstance(on, bool) else int(on)
         self._L.cvdvSetFusion(self.ctx, flags)
 
     def __del__(self):

@@ -162,7 +162,9 @@ void* cvdvGetStream(CVDVContext* ctx);
  * as one pass over the state instead of one pass per gate.  flags bit 2 (default
  * on): transforms of a register that is not the last one run as register-resident
  * column DFTs (one pass up to 2^8 points, two passes up to 2^16) instead of the
- * shared-memory tile passes.  cvdvCancelledTransforms
+ * shared-memory tile passes.  flags bit 3 (default on): a run of transforms and
+ * diagonal gates on such a register (2^8 .. 2^13 points, 2^14 in complex64) runs
+ * as one pass with each column held on chip.  cvdvCancelledTransforms
  * counts the transforms removed so far. */
 void cvdvSetFusion(CVDVContext* ctx, int flags);
 long long cvdvCancelledTransforms(CVDVContext* ctx);

@@ -214,7 +214,7 @@ def test_column_transform_matches_tile_passes(qubits, reg):
     ref = o.get_state()
     for prec, tol in (("complex128", PLAIN_TOL), ("complex64", MIXED_TOL)):
         outs = {}
-        for flags in (7, 3):
+        for flags in (15, 7, 3):
             sim = make(qubits, psi, prec)
             sim.setFusion(flags)
             _lib.load().cvdvSetTiming(sim.ctx, 1)
@@ -223,9 +223,44 @@ def test_column_transform_matches_tile_passes(qubits, reg):
             sim.d(reg, 0.4 + 0.1j)
             outs[flags] = sim.getState()
             stats = _lib.kernel_stats(sim.ctx)
-            assert (stats["col"][1] > 0) == (flags == 7), (prec, flags, stats)
+            assert (stats["col"][1] > 0) == (flags != 3), (prec, flags, stats)
             assert rel(outs[flags], ref) < tol, (prec, flags)
-        assert rel(outs[7], outs[3]) < tol
+        assert rel(outs[7], outs[3]) < tol and rel(outs[15], outs[3]) < tol
+
+
+COLUMN_GATES = [("d", (1, 0.3 + 0.2j)), ("r", (1, 0.7)), ("s", (2, 0.3)), ("bs", (1, 2, 0.4)),
+                ("h", (0, 0)), ("cd", (1, 0, 0, 0.5 + 0.1j)), ("cr", (2, 0, 0, 0.3)),
+                ("cbs", (1, 2, 0, 0, 0.25)), ("q1q2", (1, 2, 0.1)), ("cs", (1, 0, 0, 0.2)),
+                ("sheer", (2, 0.05)), ("r", (2, 2.0)), ("bs", (2, 1, -0.3)), ("d", (2, -0.2 + 0.5j)),
+                ("phaseCubic", (1, 0.01)), ("r", (1, -1.4)), ("cd", (2, 0, 0, -0.3 + 0.2j))]
+
+
+@pytest.mark.parametrize("qubits", [[1, 9, 8, 3], [1, 13, 8, 0], [1, 8, 13, 0], [1, 10, 9, 4]])
+def test_column_programs(qubits):
+    """Runs of transforms and diagonal gates on strided registers (beam splitters
+    between two of them, controls from a qubit register) as one on-chip pass per
+    run, against the oracle and against the same circuit with column programs off."""
+    from cvdv_b200 import _lib
+    qubits = [q for q in qubits if q]
+    rng = np.random.default_rng(sum(qubits))
+    n = sum(qubits)
+    psi = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    psi /= np.linalg.norm(psi)
+    o = oracle(qubits, psi)
+    run(o, COLUMN_GATES)
+    ref = o.get_state()
+    for prec, tol in (("complex128", PLAIN_TOL), ("complex64", MIXED_TOL)):
+        outs = {}
+        for flags in (15, 7):
+            sim = make(qubits, psi, prec)
+            sim.setFusion(flags)
+            _lib.load().cvdvSetTiming(sim.ctx, 1)
+            run(sim, COLUMN_GATES)
+            outs[flags] = sim.getState()
+            stats = _lib.kernel_stats(sim.ctx)
+            assert stats["col"][1] > 0, (prec, flags, stats)
+            assert rel(outs[flags], ref) < tol, (prec, flags, rel(outs[flags], ref))
+        assert rel(outs[15], outs[7]) < tol
 
 
 @pytest.mark.parametrize("n_qubits,mode_qubits", [(3, 10), (4, 13), (2, 14)])
