@@ -477,6 +477,39 @@ static void hoist_pairs_past_transforms(Context* ctx, std::vector<Stage>& st) {
   }
 }
 
+// Whether a stage acts on register r (reads or changes its amplitudes' indices
+// or phases through it).
+static bool stage_touches_reg(Context* ctx, const Stage& s, int r) {
+  const int lo = ctx->flw[r], hi = lo + ctx->q[r];
+  auto inReg = [&](int b) { return b >= lo && b < hi; };
+  switch (s.kind) {
+    case kStFft: return s.reg == r;
+    case kStPair: return inReg(s.bit);
+    case kStPerm: return s.reg == r || s.reg2 == r || (s.bit >= 0 && inReg(s.bit));
+    default:
+      for (const Term& t : s.terms) {
+        if (t.kind == kTermScalar) continue;
+        if (t.r == r || (t.kind == kTermXX && t.s == r) || (t.ctrlBit >= 0 && inReg(t.ctrlBit))) return true;
+      }
+      return false;
+  }
+}
+
+// Whether stage y may run before stage x (they commute exactly).
+static bool stage_commutes(Context* ctx, const Stage& y, const Stage& x) {
+  if (y.kind == kStDiag && x.kind == kStDiag) return true;
+  if (y.kind == kStFft) return !stage_touches_reg(ctx, x, y.reg);
+  if (y.kind != kStDiag) return false;
+  switch (x.kind) {
+    case kStFft: return !stage_touches_reg(ctx, y, x.reg);
+    case kStPair: return !terms_touch_bit(ctx, y.terms, x.bit);
+    case kStPerm:
+      return !stage_touches_reg(ctx, y, x.reg) && (x.reg2 < 0 || !stage_touches_reg(ctx, y, x.reg2)) &&
+             (x.bit < 0 || !terms_touch_bit(ctx, y.terms, x.bit));
+    default: return false;
+  }
+}
+
 bool flush(Context* ctx) {
   if (ctx->pending.empty()) return true;
   if (!ctx->initialized) {
@@ -490,18 +523,29 @@ bool flush(Context* ctx) {
   if (ctx->fuseSeq) hoist_pairs_past_transforms(ctx, stages);
   std::vector<Op> ops;
   std::vector<Term> diag;
+  // A program on one register takes every later transform of that register and
+  // every diagonal run that commutes with all the stages it would jump over
+  // (transforms of other registers, qubit gates, runs that do not fit), up to
+  // the program limits: gates on different registers are interleaved in the
+  // queue (a beam splitter, then a gate on each mode) and would otherwise cut
+  // the programs short.
+  constexpr size_t kLookahead = 256, kMaxSkipped = 96;
+  std::vector<char> taken(stages.size(), 0);
   size_t i = 0;
   while (i < stages.size()) {
+    if (taken[i]) {
+      ++i;
+      continue;
+    }
     const Stage& s = stages[i];
     if (s.kind == kStDiag) {
       diag.insert(diag.end(), s.terms.begin(), s.terms.end());
+      taken[i] = 1;
       ++i;
       continue;
     }
     const bool chain = s.kind == kStFft && ctx->colFft && col_fft_ok(ctx, s.reg);
     if (s.kind == kStFft && (row_eligible(ctx, s.reg) || col_program_ok(ctx, s.reg) || chain)) {
-      // a row program: every following FFT on this register and every diagonal
-      // run between / after them, in order, up to the program limits
       Op op;
       op.rowReg = s.reg;
       int nDiag = 0;
@@ -521,26 +565,40 @@ bool flush(Context* ctx) {
         return true;
       };
       if (!diag.empty() && !addDiag(diag)) {
-        run_leftover(ctx, diag);  // unusual: the leading run is too large; run it alone
+        // unusual: the leading run is too large for a program; it runs on its own first
+        ops.push_back(Op{});
+        ops.back().pre = diag;
         op.row.clear();
         nDiag = 0;
       }
       diag.clear();
-      size_t j = i;
-      while (j < stages.size()) {
+      std::vector<size_t> skipped;
+      for (size_t j = i; j < stages.size() && j < i + kLookahead; ++j) {
+        if (taken[j]) continue;
         const Stage& t = stages[j];
-        if (t.kind == kStFft && t.reg == s.reg) {
+        bool free = true;
+        for (size_t k : skipped)
+          if (!stage_commutes(ctx, t, stages[k])) {
+            free = false;
+            break;
+          }
+        bool took = false;
+        if (free && t.kind == kStFft && t.reg == s.reg) {
           if ((int)op.row.size() + 2 > kMaxRowOps) break;
           op.row.push_back({kRowFft, t.dir, {}});
-        } else if (t.kind == kStDiag) {
-          if (!addDiag(t.terms)) break;
-        } else {
-          break;
+          took = true;
+        } else if (free && t.kind == kStDiag) {
+          took = addDiag(t.terms);
         }
-        ++j;
+        if (took) {
+          taken[j] = 1;
+        } else {
+          skipped.push_back(j);
+          if (skipped.size() > kMaxSkipped) break;
+        }
       }
       ops.push_back(std::move(op));
-      i = j;
+      ++i;
       continue;
     }
     Op op;
@@ -548,6 +606,7 @@ bool flush(Context* ctx) {
     op.pre = diag;
     ops.push_back(std::move(op));
     diag.clear();
+    taken[i] = 1;
     ++i;
   }
   if (ops.empty()) return run_leftover(ctx, diag);
