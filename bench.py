@@ -260,7 +260,7 @@ def run_gpu(args, world, rank, local):
     # Every kernel of this workload is one read + write of the state: the
     # algorithmic bytes of a launch are 2 * 2^n * 16 B (complex128).
     alg_bytes = 2 * n_amp * 16
-    KNAME = {"seq": "k_seq (qubit-gate sequence: H, conditional phase in p and Rz on up to four qubits per pass)",
+    KNAME = {"seq": "k_seq (qubit-gate sequence: H, conditional phase in p and Rz on up to five qubits per pass)",
              "pair": "k_pair (one qubit gate with the neighbouring diagonal runs)",
              "fft_pass": "k_row (row program: mode DFT + diagonal runs; 2^14-point rows on a 2-CTA cluster of 512-thread CTAs)"}
 
@@ -345,7 +345,7 @@ def run_gpu(args, world, rank, local):
                 "d2h_bytes_per_step": d2h, "includes": "init from host arrays + 2 prep gates + 42 gates + 14 marginals"},
         "norm_after": norm,
         "queue_fusion": "FtP2Q/FtQ2P pairs separated only by gates on other registers are cancelled "
-                        "(exact identity) and chains of qubit gates on up to four qubits run as one pass; "
+                        "(exact identity) and chains of qubit gates on up to five qubits run as one pass; "
                         "every_transform_executed is the run with both off (one pass per gate)",
         "every_transform_executed": {"value": G * world / (msnf * 1e-3), "ms_per_step": msnf,
                                      "gpu_launches": int(launchesnf), "kernels": krnf, "norm_after": normnf},
@@ -357,7 +357,7 @@ def run_gpu(args, world, rank, local):
         threads = os.cpu_count() or 1
         times = cpu_oracle_gates(circ, [0, 1, 2], threads)
         line["cpu_baseline"] = {"value": 3 / sum(times), "unit": UNIT, "cores": threads, "kind": "port",
-                                "sample": "round 1 (H, cd, Rz) of the circuit at full 2^28 size on the CPU oracle"}
+                                "sample": "the first (H, cd, Rz) triple of the circuit at full 2^28 size on the CPU oracle"}
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -408,15 +408,16 @@ def batched_c4(args):
 
 
 def gaussian_c3(args):
-    """Two modes [13, 13] (2^26 amplitudes), complex128 and complex64: layers of (beam splitter,
-    rotation of each mode, displacement of each mode); 20 layers per step, then the Wigner
-    function of mode 0 (8192 x 8192, read back)."""
+    """Two modes [13, 13] (2^26 amplitudes; [12, 12] for --workload small), complex128 and
+    complex64: layers of (beam splitter, rotation of each mode, displacement of each mode);
+    20 layers per step, then the Wigner function of mode 0 (read back)."""
     import torch
     from cvdv_b200 import CudaCvdv, _lib
     from cvdv_b200 import workloads as W
     L = _lib.load()
     layers = 20
-    circ = W.gaussian_network(layers=layers)
+    mq = 13 if args.workload == "full" else 12
+    circ = W.gaussian_network(layers=layers, mode_qubits=mq)
     out = {"unit": "layers/s", "layers_per_step": layers, "gates_per_layer": len(circ["gates"]) // layers}
     for prec in ("complex128", "complex64"):
         sim = CudaCvdv(circ["qubits"], precision=prec, check_errors=True)
@@ -434,10 +435,24 @@ def gaussian_c3(args):
         e1.record(stream)
         e1.synchronize()
         ms = e0.elapsed_time(e1) / (reps * layers)
+        # per-kind kernel times of one more step, with per-launch events on
+        L.cvdvSetTiming(sim.ctx, 1)
+        _lib.kernel_stats(sim.ctx)
+        W.apply(sim, circ["gates"])
+        L.cvdvFlush(sim.ctx)
+        st = _lib.kernel_stats(sim.ctx)
+        L.cvdvSetTiming(sim.ctx, 0)
+        kern = {k: {"ms_per_layer": v[0] / layers, "launches_per_layer": v[1] / layers}
+                for k, v in st.items() if v[1]}
+        state_bytes = (16 if prec == "complex128" else 8) << sum(circ["qubits"])
+        if "col" in kern:  # one column pass reads and writes the state once
+            avg = kern["col"]["ms_per_layer"] / kern["col"]["launches_per_layer"]
+            kern["col"]["achieved_gbs"] = 2 * state_bytes / (avg * 1e-3) / 1e9
         t0 = time.perf_counter()
         w = sim.getWigner(0)
         wig_s = time.perf_counter() - t0
-        out[prec] = {"value": 1e3 / ms, "ms_per_layer": ms, "wigner_s": wig_s, "wigner_shape": list(w.shape)}
+        out[prec] = {"value": 1e3 / ms, "ms_per_layer": ms, "wigner_s": wig_s, "wigner_shape": list(w.shape),
+                     "kernels": kern}
         del sim
         torch.cuda.empty_cache()
     out["value"] = out["complex128"]["value"]
@@ -486,13 +501,19 @@ def main():
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched-circuits and variational-gradient measurements")
     ap.add_argument("--workload", default="full", choices=["full", "small"],
-                    help="small: 10 qubit registers + the 2^14 mode (2^24 amplitudes), for ncu")
+                    help="small: 10 qubit registers + the 2^14 mode (2^24 amplitudes), and the two-mode "
+                         "network at [12, 12], for ncu")
+    ap.add_argument("--extra", default=None, choices=["c3", "c4", "c5"],
+                    help="run only that extra measurement (one GPU) and print its JSON, for profiling")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     world, rank, local = dist_init()
     try:
-        if args.impl == "reference":
+        if args.extra:
+            fn = {"c3": gaussian_c3, "c4": batched_c4, "c5": variational_c5}[args.extra]
+            print(json.dumps({"extra": args.extra, **fn(args)}), flush=True)
+        elif args.impl == "reference":
             run_reference(args, world, rank)
         else:
             run_gpu(args, world, rank, local)
