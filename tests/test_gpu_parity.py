@@ -263,6 +263,74 @@ def test_column_programs(qubits):
         assert rel(outs[15], outs[7]) < tol
 
 
+def _random_multimode_circuit(rng, qubits, n_gates):
+    """Gates of every kind on a layout [qubit register, mode, mode, (mode)]: single-
+    and two-mode gates, controlled ones from the qubits, qubit gates, quarter turns
+    (transforms and parity permutations) and half-turn beam splitters (swaps)."""
+    modes = list(range(1, len(qubits)))
+    seq = []
+    for _ in range(n_gates):
+        g = int(rng.integers(14))
+        m = int(modes[rng.integers(len(modes))])
+        m2 = int(modes[rng.integers(len(modes))])
+        k = int(rng.integers(qubits[0]))
+        th = float(rng.uniform(-np.pi, np.pi))
+        a = complex(rng.normal(0, 0.5), rng.normal(0, 0.5))
+        if g == 0:
+            seq.append(("d", (m, a)))
+        elif g == 1:
+            seq.append(("r", (m, th)))
+        elif g == 2:
+            seq.append(("s", (m, float(rng.uniform(-0.4, 0.4)))))
+        elif g == 3 and m != m2:
+            seq.append(("bs", (m, m2, th if qubits[m] == qubits[m2] else th / 8)))
+        elif g == 4:
+            seq.append(("cd", (m, 0, k, a)))
+        elif g == 5:
+            seq.append(("cr", (m, 0, k, th)))
+        elif g == 6 and m != m2:
+            seq.append(("cbs", (m, m2, 0, k, th / 4)))
+        elif g == 7:
+            seq.append(("h", (0, k)))
+        elif g == 8:
+            seq.append(("rx", (0, k, th)))
+        elif g == 9:
+            seq.append(("sheer", (m, float(rng.uniform(-0.2, 0.2)))))
+        elif g == 10 and m != m2:
+            seq.append(("q1q2", (m, m2, float(rng.uniform(-0.1, 0.1)))))
+        elif g == 11:
+            seq.append(("cs", (m, 0, k, float(rng.uniform(-0.3, 0.3)))))
+        elif g == 12:
+            seq.append((("ftQ2P", "ftP2Q")[int(rng.integers(2))], (m,)))
+        else:
+            seq.append(("phaseCubic", (m, float(rng.uniform(-0.02, 0.02)))))
+    return seq
+
+
+@pytest.mark.parametrize("qubits", [[2, 9, 9], [1, 8, 6, 5], [2, 13, 5], [1, 5, 12]])
+def test_random_multimode_circuits(qubits):
+    """Random circuits over several modes: the planner's look-ahead (programs that
+    jump over commuting stages), column chains and row programs against the oracle,
+    and against the same circuit with every queue optimisation off."""
+    rng = np.random.default_rng(sum(qubits) * 13 + len(qubits))
+    n = sum(qubits)
+    psi = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    psi /= np.linalg.norm(psi)
+    seq = _random_multimode_circuit(rng, qubits, 60)
+    o = oracle(qubits, psi)
+    run(o, seq)
+    ref = o.get_state()
+    for prec, tol in (("complex128", PLAIN_TOL), ("complex64", MIXED_TOL)):
+        outs = {}
+        for fusion in (True, False):
+            sim = make(qubits, psi, prec)
+            sim.setFusion(fusion)
+            run(sim, seq)
+            outs[fusion] = sim.getState()
+            assert rel(outs[fusion], ref) < tol, (prec, fusion, rel(outs[fusion], ref))
+        assert rel(outs[True], outs[False]) < tol
+
+
 @pytest.mark.parametrize("n_qubits,mode_qubits", [(3, 10), (4, 13), (2, 14)])
 def test_state_transfer_scaled(n_qubits, mode_qubits):
     """The headline circuit at reduced size, plain and mixed."""
