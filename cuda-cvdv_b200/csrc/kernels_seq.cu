@@ -171,8 +171,10 @@ __device__ __forceinline__ void seq_pair_lanes(C* v, int kind, const Mat2 m, int
 
 // A site of 2^NB amplitudes is held by 2^SPLIT consecutive lanes: the top SPLIT
 // selected bits pick the lane, the other NB - SPLIT the register.  Gates on a
-// lane bit exchange partners with warp shuffles.
-template <typename C, int NB, int SPLIT, typename IDX>
+// lane bit exchange partners with warp shuffles.  GEN = false: the sequence's 2x2
+// gates are all Hadamard-type, and the general-matrix paths are compiled out
+// (fewer live registers, fewer spills of the site).
+template <typename C, int NB, int SPLIT, typename IDX, bool GEN>
 __global__ void __launch_bounds__(256, 2) k_seq(C* __restrict__ st, IDX nSites,
                                                const __grid_constant__ SeqProgram P) {
   constexpr int NBL = NB - SPLIT;  // bits held in registers
@@ -215,17 +217,27 @@ __global__ void __launch_bounds__(256, 2) k_seq(C* __restrict__ st, IDX nSites,
     for (int o = 0; o < P.nOps; ++o) {
       const SeqOp& op = P.ops[o];
       if (op.kind != kSeqDiag) {
-        const Mat2 mm{op.m[0], op.m[1], op.m[2], op.m[3]};
-        if (op.kind == kSeqPairH) sc *= (R)mm.m0.x;
-        if (SPLIT > 0 && op.bit >= NBL) {
-          const int lb = op.bit - NBL;
-          seq_pair_lanes<C, KL>(v, op.kind, mm, 1 << lb, (part >> lb) & 1);
-        } else if (op.kind == kSeqPairH) {
-          SEQ_BIT_SWITCH(op.bit, (seq_pair_h<C, NBL, B_>(v)))
-        } else if (op.kind == kSeqPairReal) {
-          SEQ_BIT_SWITCH(op.bit, (seq_pair_real<C, NBL, B_>(v, mm)))
+        if constexpr (!GEN) {  // Hadamard-type pairs only
+          sc *= (R)op.m[0].x;
+          if (SPLIT > 0 && op.bit >= NBL) {
+            const int lb = op.bit - NBL;
+            seq_pair_lanes<C, KL>(v, kSeqPairH, Mat2{}, 1 << lb, (part >> lb) & 1);
+          } else {
+            SEQ_BIT_SWITCH(op.bit, (seq_pair_h<C, NBL, B_>(v)))
+          }
         } else {
-          SEQ_BIT_SWITCH(op.bit, (seq_pair<C, NBL, B_>(v, mm)))
+          const Mat2 mm{op.m[0], op.m[1], op.m[2], op.m[3]};
+          if (op.kind == kSeqPairH) sc *= (R)mm.m0.x;
+          if (SPLIT > 0 && op.bit >= NBL) {
+            const int lb = op.bit - NBL;
+            seq_pair_lanes<C, KL>(v, op.kind, mm, 1 << lb, (part >> lb) & 1);
+          } else if (op.kind == kSeqPairH) {
+            SEQ_BIT_SWITCH(op.bit, (seq_pair_h<C, NBL, B_>(v)))
+          } else if (op.kind == kSeqPairReal) {
+            SEQ_BIT_SWITCH(op.bit, (seq_pair_real<C, NBL, B_>(v, mm)))
+          } else {
+            SEQ_BIT_SWITCH(op.bit, (seq_pair<C, NBL, B_>(v, mm)))
+          }
         }
       } else {
         const SeqDiag& D = P.diag[op.diag];
@@ -318,7 +330,10 @@ int seq_max_bits(Context* ctx) {
 
 template <typename C, int NB, int SPLIT, typename IDX>
 static void seq_go(Context* ctx, unsigned blocks, uint64_t nSites, const SeqProgram& P) {
-  k_seq<C, NB, SPLIT, IDX><<<blocks, 256, 0, ctx->stream>>>((C*)ctx->state(), (IDX)nSites, P);
+  bool gen = false;
+  for (int o = 0; o < P.nOps; ++o) gen |= P.ops[o].kind == kSeqPair || P.ops[o].kind == kSeqPairReal;
+  if (gen) k_seq<C, NB, SPLIT, IDX, true><<<blocks, 256, 0, ctx->stream>>>((C*)ctx->state(), (IDX)nSites, P);
+  else k_seq<C, NB, SPLIT, IDX, false><<<blocks, 256, 0, ctx->stream>>>((C*)ctx->state(), (IDX)nSites, P);
 }
 
 template <typename C, typename IDX>
