@@ -10,9 +10,9 @@ namespace cvdv {
 
 // shared-memory position of element e of a row: one padding slot every 16
 // (the radix-16 stride), which keeps the strided butterfly accesses conflict-free
-template <typename C>
+template <typename C, int LOGP = 4>
 __device__ __forceinline__ int rpad(int e) {
-  return e + (e >> 4);
+  return e + (e >> LOGP);
 }
 
 // ---------------------------------------------------------------- butterflies
@@ -107,9 +107,45 @@ __device__ __forceinline__ void bf16(C* v) {
   }
 }
 
+// radix 32 = 2 x 16: y[k] = E[k] + w32^k O[k], y[k + 16] = E[k] - w32^k O[k] with E, O
+// the 16-point DFTs of the even and odd inputs (complex64 rows, 32 amplitudes a thread)
+template <typename C, int DIR>
+__device__ __forceinline__ void bf32(C* v) {
+  using T = decltype(v[0].x);
+  // cos(k pi / 16), k = 0..8
+  constexpr double cs[9] = {1.0,
+                            0.98078528040323044913,
+                            0.92387953251128675613,
+                            0.83146961230254523708,
+                            0.70710678118654752440,
+                            0.55557023301960222474,
+                            0.38268343236508977173,
+                            0.19509032201612826785,
+                            0.0};
+  C e[16], o[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    e[i] = v[2 * i];
+    o[i] = v[2 * i + 1];
+  }
+  bf16<C, DIR>(e);
+  bf16<C, DIR>(o);
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    // w32^k = cos(k pi / 16) - DIR i sin(k pi / 16)
+    const T c = (T)(k <= 8 ? cs[k] : -cs[16 - k]);
+    const T sn = (T)(k <= 8 ? cs[8 - k] : cs[k - 8]);
+    const T si = DIR > 0 ? -sn : sn;
+    const C t = mk(o[k].x * c - o[k].y * si, o[k].x * si + o[k].y * c);
+    v[k] = cadd(e[k], t);
+    v[k + 16] = csub(e[k], t);
+  }
+}
+
 template <typename C, int DIR, int RHO>
 __device__ __forceinline__ void bfly(C* v) {
-  if constexpr (RHO == 16) bf16<C, DIR>(v);
+  if constexpr (RHO == 32) bf32<C, DIR>(v);
+  else if constexpr (RHO == 16) bf16<C, DIR>(v);
   else if constexpr (RHO == 8) bf8<C, DIR>(v);
   else if constexpr (RHO == 4) bf4<C, DIR>(v[0], v[1], v[2], v[3]);
   else bf2<C, DIR>(v[0], v[1]);
@@ -137,18 +173,27 @@ __device__ __forceinline__ void rr_butterflies(C (&v)[1 << LOGE], int t, const d
     if constexpr (LOGNS > 0) {
       const int jm = (t + b * TPR) & ((1 << LOGNS) - 1);
       // w_{ns R}^{jm u} = w_M^{(jm u) << (LOGM - LOGNS - LOGRAD)}; powers as a tree
-      C w[RAD];
+      // powers w^u as a tree (w^(u + 2^j) = w^u w^(2^j)); for radix 32 the upper
+      // half is formed as it is applied, so only 17 powers are live at once
+      constexpr int RT = RAD > 16 ? 16 : RAD;
+      C w[RT + 1];
       w[1] = tw2<C, DIR>(lo, hi, jm << (LOGM - LOGNS - LOGRAD));
 #pragma unroll
-      for (int p = 1; p < RAD / 2; p <<= 1) {
+      for (int p = 1; p < RT / 2; p <<= 1) {
         w[2 * p] = cmul(w[p], w[p]);
 #pragma unroll
         for (int u = 1; u < p; ++u) w[p + u] = cmul(w[p], w[u]);
       }
 #pragma unroll
-      for (int u = RAD / 2 + 1; u < RAD; ++u) w[u] = cmul(w[RAD / 2], w[u - RAD / 2]);
+      for (int u = RT / 2 + 1; u < RT; ++u) w[u] = cmul(w[RT / 2], w[u - RT / 2]);
+      if constexpr (RAD > 16) w[16] = cmul(w[8], w[8]);
 #pragma unroll
-      for (int u = 1; u < RAD; ++u) x[u] = cmul(x[u], w[u]);
+      for (int u = 1; u < RT; ++u) x[u] = cmul(x[u], w[u]);
+      if constexpr (RAD > 16) {
+        x[16] = cmul(x[16], w[16]);
+#pragma unroll
+        for (int u = 17; u < RAD; ++u) x[u] = cmul(x[u], cmul(w[16], w[u - 16]));
+      }
     }
     bfly<C, DIR, RAD>(x);
 #pragma unroll
@@ -157,7 +202,9 @@ __device__ __forceinline__ void rr_butterflies(C (&v)[1 << LOGE], int t, const d
 }
 
 // outputs of a stage to their autosorted positions, then the next stage's inputs
-template <typename C, int LOGM, int LOGRAD, int LOGNS, int LOGE>
+// (padding period 2^LOGP elements: 16 for radix-16 stages, 32 for radix-32 ones,
+// so the first stage's writes at stride RAD stay free of bank conflicts)
+template <typename C, int LOGM, int LOGRAD, int LOGNS, int LOGE, int LOGP = 4>
 __device__ __forceinline__ void rr_exchange(C (&v)[1 << LOGE], C* smrow, int t) {
   constexpr int E = 1 << LOGE, RAD = 1 << LOGRAD, NB = E / RAD, TPR = 1 << (LOGM - LOGE);
 #pragma unroll
@@ -165,24 +212,27 @@ __device__ __forceinline__ void rr_exchange(C (&v)[1 << LOGE], C* smrow, int t) 
     const int j = t + b * TPR;
     const int y = ((j >> LOGNS) << (LOGNS + LOGRAD)) + (j & ((1 << LOGNS) - 1));
 #pragma unroll
-    for (int u = 0; u < RAD; ++u) smrow[rpad<C>(y + (u << LOGNS))] = v[b + NB * u];
+    for (int u = 0; u < RAD; ++u) smrow[rpad<C, LOGP>(y + (u << LOGNS))] = v[b + NB * u];
   }
   __syncthreads();
 #pragma unroll
-  for (int k = 0; k < E; ++k) v[k] = smrow[rpad<C>(t + k * TPR)];
+  for (int k = 0; k < E; ++k) v[k] = smrow[rpad<C, LOGP>(t + k * TPR)];
   __syncthreads();
 }
 
+// The stages of one transform: radix 16 (radix 32 with 32 amplitudes a thread),
+// then the remaining radix.  The shared row holds at least M + M/16 elements.
 template <typename C, int DIR, int LOGM, int S, int LOGE = 4>
 __device__ __forceinline__ void rr_stages(C (&v)[1 << LOGE], C* smrow, int t, const double2* lo,
                                           const double2* hi) {
-  constexpr int N16 = LOGM / 4, REM = LOGM % 4;
-  if constexpr (S < N16) {
-    rr_butterflies<C, DIR, LOGM, 4, 4 * S, LOGE>(v, t, lo, hi);
-    if constexpr (S + 1 < N16 || REM) rr_exchange<C, LOGM, 4, 4 * S, LOGE>(v, smrow, t);
+  constexpr int LR = LOGE >= 5 ? 5 : 4;  // log2 of the full stages' radix
+  constexpr int NF = LOGM / LR, REM = LOGM % LR;
+  if constexpr (S < NF) {
+    rr_butterflies<C, DIR, LOGM, LR, LR * S, LOGE>(v, t, lo, hi);
+    if constexpr (S + 1 < NF || REM) rr_exchange<C, LOGM, LR, LR * S, LOGE, LR>(v, smrow, t);
     rr_stages<C, DIR, LOGM, S + 1, LOGE>(v, smrow, t, lo, hi);
   } else if constexpr (REM > 0) {
-    rr_butterflies<C, DIR, LOGM, REM, 4 * N16, LOGE>(v, t, lo, hi);
+    rr_butterflies<C, DIR, LOGM, REM, LR * NF, LOGE>(v, t, lo, hi);
   }
 }
 
