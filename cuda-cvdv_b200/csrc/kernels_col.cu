@@ -5,8 +5,8 @@
 // amplitudes below it).  A "column" is one transform line: fixed outer and inner
 // indices, stride S along the register.  A CTA of 256 threads takes W adjacent
 // columns (adjacent inner indices, so every load and store instruction covers W
-// consecutive amplitudes) and keeps each column's L points in registers, 16 per
-// thread; the Stockham stages of the row kernels (row_fft.cuh) exchange through
+// consecutive amplitudes) and keeps each column's L points in registers, 16 (or
+// 8) per thread; the Stockham stages of the row kernels (row_fft.cuh) exchange through
 // one padded shared-memory line per column.  A pass runs a small program on its
 // columns: DFTs, diagonal runs (factor lists of the flat index) and the four-step
 // twiddle.
@@ -54,33 +54,42 @@ struct ColPass {
   FactorList diag[kMaxColDiags];  // evaluated at input addresses before the first DFT, output ones after
 };
 
-template <int LOGL>
+// CE: log2 of the points a thread holds (16 or 8); the shared line of a column is
+// padded once per radix (16 or 8 points) and has an odd length, so the W columns
+// of a warp fall on distinct banks
+template <int LOGL, int CE>
 struct ColShape {
-  static constexpr int L = 1 << LOGL, TPC = L >> 4, W = kColThreads / TPC;
-  static constexpr int RS = (L + (L >> 4)) | 1;  // odd: the W columns of a warp fall on distinct banks
+  static constexpr int E = 1 << CE, L = 1 << LOGL, TPC = L >> CE, W = kColThreads / TPC;
+  static constexpr int RS = (L + (L >> (CE >= 4 ? 4 : 3))) | 1;
   static constexpr int HI = L >= 64 ? (L >> 6) : 1;
 };
+
+// points per thread of the column kernel (log2): 8 in complex128, so that three
+// CTAs fit an SM (24 warps instead of 16; 0.71 against 0.80 ms per pass of a
+// 2^26-amplitude state), 16 in complex64
+template <typename C> struct ColCE { static constexpr int v = 4; };
+template <> struct ColCE<double2> { static constexpr int v = 3; };
 
 // Pass shapes: the first half of a transform (diagonal runs on the loads, DFT,
 // four-step twiddle), a shared middle pass (DFT, runs, DFT, twiddle), the second
 // half (DFT, runs on the stores), or a whole run on a short register (the op list).
 enum ColKind : int { kColFirst = 0, kColMiddle = 1, kColLast = 2, kColWhole = 3 };
 
-template <typename C, int LOGL>
-__device__ __forceinline__ void col_diags(C (&v)[16], const ColPass& P, uint64_t b, uint64_t ax, int t) {
-  constexpr int TPC = ColShape<LOGL>::TPC;
+template <typename C, int LOGL, int CE>
+__device__ __forceinline__ void col_diags(C (&v)[1 << CE], const ColPass& P, uint64_t b, uint64_t ax, int t) {
+  constexpr int TPC = ColShape<LOGL, CE>::TPC;
   for (int d = 0; d < P.nDiag; ++d) {
 #pragma unroll
-    for (int k = 0; k < 16; ++k)
+    for (int k = 0; k < (1 << CE); ++k)
       v[k] = cmul(v[k], fromd<C>(eval_factor(P.diag[d], b + (uint64_t)(t + TPC * k) * ax)));
   }
 }
 
-template <typename C, int LOGL, int KIND, int D1, int D2>
-__global__ void __launch_bounds__(kColThreads, 2)
+template <typename C, int LOGL, int KIND, int D1, int D2, int CE = ColCE<C>::v>
+__global__ void __launch_bounds__(kColThreads, CE >= 4 ? 2 : 3)
     k_colr(const C* __restrict__ in, C* __restrict__ out, const __grid_constant__ ColPass P) {
-  using S = ColShape<LOGL>;
-  constexpr int TPC = S::TPC, W = S::W;
+  using S = ColShape<LOGL, CE>;
+  constexpr int TPC = S::TPC, W = S::W, E = S::E;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
   double2* loL = reinterpret_cast<double2*>(sm + (size_t)W * S::RS);  // w_L^e, e < 64
@@ -115,10 +124,10 @@ __global__ void __launch_bounds__(kColThreads, 2)
   const uint64_t bIn = i + mid * P.midIn + o * P.outerIn;
   const uint64_t bOut = i + mid * P.midOut + o * P.outerOut;
   C* smcol = sm + (size_t)w * S::RS;
-  C v[16];
+  C v[E];
   // the first half's diagonal runs ride on the loads, the last half's on the stores
 #pragma unroll
-  for (int k = 0; k < 16; ++k) {
+  for (int k = 0; k < E; ++k) {
     const uint64_t a = bIn + (uint64_t)(t + TPC * k) * P.axisIn;
     v[k] = in[a];
     if constexpr (KIND == kColFirst)
@@ -129,26 +138,26 @@ __global__ void __launch_bounds__(kColThreads, 2)
     for (int p = 0; p < P.nOps; ++p) {
       const ColOp& op = P.ops[p];
       if (op.kind == kColDft) {
-        if (op.dir > 0) rr_stages<C, 1, LOGL, 0, 4>(v, smcol, t, loL, hiL);
-        else rr_stages<C, -1, LOGL, 0, 4>(v, smcol, t, loL, hiL);
+        if (op.dir > 0) rr_stages<C, 1, LOGL, 0, CE>(v, smcol, t, loL, hiL);
+        else rr_stages<C, -1, LOGL, 0, CE>(v, smcol, t, loL, hiL);
       } else {
         const FactorList& F = P.diag[op.diag];
 #pragma unroll
-        for (int k = 0; k < 16; ++k)
+        for (int k = 0; k < E; ++k)
           v[k] = cmul(v[k], fromd<C>(eval_factor(F, bOut + (uint64_t)(t + TPC * k) * P.axisOut)));
       }
     }
   } else {
-    rr_stages<C, D1, LOGL, 0, 4>(v, smcol, t, loL, hiL);
+    rr_stages<C, D1, LOGL, 0, CE>(v, smcol, t, loL, hiL);
     if constexpr (KIND == kColMiddle) {
-      col_diags<C, LOGL>(v, P, bOut, P.axisOut, t);
-      rr_stages<C, D2, LOGL, 0, 4>(v, smcol, t, loL, hiL);
+      col_diags<C, LOGL, CE>(v, P, bOut, P.axisOut, t);
+      rr_stages<C, D2, LOGL, 0, CE>(v, smcol, t, loL, hiL);
     }
   }
   constexpr int DT = KIND == kColMiddle ? D2 : D1;  // direction of the four-step twiddle
   const int nMask = (1 << P.logN) - 1;
 #pragma unroll
-  for (int k = 0; k < 16; ++k) {
+  for (int k = 0; k < E; ++k) {
     const int m = t + TPC * k;
     const uint64_t a = bOut + (uint64_t)m * P.axisOut;
     C x = v[k];
@@ -164,7 +173,7 @@ __global__ void __launch_bounds__(kColThreads, 2)
 
 template <typename C, int LOGL, int KIND, int D1, int D2>
 static cudaError_t col_launch_t(Context* ctx, const ColPass& P) {
-  using S = ColShape<LOGL>;
+  using S = ColShape<LOGL, ColCE<C>::v>;
   const int nHiN = P.logN >= 6 ? 1 << (P.logN - 6) : 1;
   const size_t smem = (size_t)S::W * S::RS * sizeof(C) + (64 + S::HI + 64 + nHiN) * sizeof(double2);
   const unsigned grid = (unsigned)(P.nCols / S::W);

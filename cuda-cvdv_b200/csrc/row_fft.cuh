@@ -220,12 +220,13 @@ __device__ __forceinline__ void rr_exchange(C (&v)[1 << LOGE], C* smrow, int t) 
   __syncthreads();
 }
 
-// The stages of one transform: radix 16 (radix 32 with 32 amplitudes a thread),
-// then the remaining radix.  The shared row holds at least M + M/16 elements.
+// The stages of one transform: radix 16 (radix 32 with 32 amplitudes a thread,
+// radix 8 with 8), then the remaining radix.  The shared row holds at least
+// M + M/16 elements (M + M/8 with 8 amplitudes a thread).
 template <typename C, int DIR, int LOGM, int S, int LOGE = 4>
 __device__ __forceinline__ void rr_stages(C (&v)[1 << LOGE], C* smrow, int t, const double2* lo,
                                           const double2* hi) {
-  constexpr int LR = LOGE >= 5 ? 5 : 4;  // log2 of the full stages' radix
+  constexpr int LR = LOGE >= 5 ? 5 : (LOGE == 3 ? 3 : 4);  // log2 of the full stages' radix
   constexpr int NF = LOGM / LR, REM = LOGM % LR;
   if constexpr (S < NF) {
     rr_butterflies<C, DIR, LOGM, LR, LR * S, LOGE>(v, t, lo, hi);
