@@ -53,18 +53,51 @@ def peaks():
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """SM clock and clock-event reasons sampled DURING the timed region: NVML read
+    every 5 ms from a background thread (the region lasts tens of milliseconds, too
+    short for nvidia-smi's sampling); nvidia-smi at 200 ms if NVML is missing.
+    Read-only queries: no clock or power setting is touched."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+               "sw_power_cap": 0x4}
 
     def __init__(self, gpu: int):
         self.gpu = gpu
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         self.p = None
+        self.thread = None
+        self.samples = []
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(gpu)
+        except Exception:
+            self.nvml = None
+
+    def _poll(self):
+        nv = self.nvml
+        while not self.done:
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                smax = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+                get = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                    nv.nvmlDeviceGetCurrentClocksThrottleReasons
+                self.samples.append((sm, smax, int(get(self.h))))
+            except Exception:
+                pass
+            time.sleep(0.005)
 
     def start(self):
+        if self.nvml is not None:
+            import threading
+            self.done = False
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
                                        "--format=csv,noheader,nounits", "-lms", "200"],
@@ -73,6 +106,14 @@ class Clocks:
             self.p = None
 
     def stop(self):
+        if self.thread is not None:
+            self.done = True
+            self.thread.join(timeout=5)
+            sm = [x[0] for x in self.samples]
+            reasons = sorted(k for k, bit in self.REASONS.items() if any(x[2] & bit for x in self.samples))
+            return {"sm_mhz": statistics.median(sm) if sm else None,
+                    "sm_max_mhz": max(x[1] for x in self.samples) if sm else None,
+                    "reasons": reasons, "samples": len(sm), "source": "nvml, 5 ms"}
         if self.p is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         time.sleep(0.3)
@@ -96,7 +137,7 @@ class Clocks:
                 continue
         os.unlink(self.f.name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
 _BACKEND = "nccl"
@@ -282,7 +323,7 @@ def run_gpu(args, world, rank, local):
     # scaled by the 16x larger state: the kernels stream the state once per launch,
     # so their traffic grows with the rows / sites processed.
     ncu_traffic_2p24 = {"fft_pass": ((269.3 + 219.8) + (269.1 + 222.2)) / 2 * 1e6,  # k_rowc, two launches
-                        "seq": (272.4 + 214.5) * 1e6}                                  # k_seq<double2, 5, 1>
+                        "seq": (272.5 + 211.6) * 1e6}                                  # k_seq<double2, 5, 1, u32, 0>
     scale = n_amp / float(1 << 24)
     traffic = ncu_traffic_2p24[dom] * scale if (dom in ncu_traffic_2p24 and args.workload == "full") else None
     achieved = kr[dom]["achieved_gbs"]
