@@ -8,7 +8,8 @@
 // uncoalesced gathers, O(N^2 M).  Here the same sum is read off the reduced
 // density matrix rho[a][b] = sum_o psi_o[a] conj(psi_o[b]), formed as a tiled
 // Hermitian GEMM (upper-triangle tiles only, FP64 accumulation, shared-memory
-// operand tiles), then G[i,k] = rho[i-kd][i+kd] is gathered, a batched inverse
+// operand tiles, only the entries with a + b even that the gather reads), then
+// G[i,k] = rho[i-kd][i+kd] is gathered, a batched inverse
 // FFT runs along k, and a transposing epilogue applies the phase correction,
 // the fftshift and dx/pi.
 //
@@ -44,6 +45,10 @@ __device__ __forceinline__ uint64_t slice_addr(uint64_t o, uint64_t a, int flw, 
 constexpr int kRT = 64;   // output tile
 constexpr int kRK = 16;   // slices per k-step
 
+// The Wigner gather reads rho[a][b] only at a + b even (a = i - kd, b = i + kd), so
+// the GEMM forms the two same-parity blocks, a = 2 a' + par and b = 2 b' + par
+// (par = blockIdx.z), each an N/2 x N/2 Hermitian product: a quarter of the full
+// N x N x M work instead of half.  Tile indices below are in the halved index.
 template <typename C>
 __global__ void __launch_bounds__(256) k_rho(const C* __restrict__ st, int N, int q, int flw,
                                             uint64_t M, double2* __restrict__ rho, int aFast) {
@@ -51,6 +56,7 @@ __global__ void __launch_bounds__(256) k_rho(const C* __restrict__ st, int N, in
   if (ta > tb) return;  // Hermitian: upper tiles only
   __shared__ double2 sA[kRK][kRT + 1];
   __shared__ double2 sB[kRK][kRT + 1];
+  const int par = blockIdx.z, Nh = N >> 1;
   const int a0 = ta * kRT, b0 = tb * kRT;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   double2 acc[4][4];
@@ -71,8 +77,8 @@ __global__ void __launch_bounds__(256) k_rho(const C* __restrict__ st, int N, in
       uint64_t o = o0 + kk;
       double2 va = make_double2(0.0, 0.0), vb = make_double2(0.0, 0.0);
       if (o < M) {
-        if (a0 + a < N) va = tod2<C>(st[slice_addr(o, a0 + a, flw, q)]);
-        if (b0 + a < N) vb = tod2<C>(st[slice_addr(o, b0 + a, flw, q)]);
+        if (a0 + a < Nh) va = tod2<C>(st[slice_addr(o, 2 * (a0 + a) + par, flw, q)]);
+        if (b0 + a < Nh) vb = tod2<C>(st[slice_addr(o, 2 * (b0 + a) + par, flw, q)]);
       }
       sA[kk][a] = va;
       sB[kk][a] = vb;
@@ -101,7 +107,7 @@ __global__ void __launch_bounds__(256) k_rho(const C* __restrict__ st, int N, in
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       int a = a0 + ty + 16 * i, b = b0 + tx + 16 * j;
-      if (a < N && b < N) rho[(size_t)a * N + b] = acc[i][j];
+      if (a < Nh && b < Nh) rho[(size_t)(2 * a + par) * N + 2 * b + par] = acc[i][j];
     }
 }
 
@@ -263,7 +269,8 @@ static bool wigner_device(Context* c, int r, double* out, double2* complexOut, d
   double2* rho = work;
   double2* G = work + NN;
   double2* T = work + 2 * NN;
-  dim3 g((N + kRT - 1) / kRT, (N + kRT - 1) / kRT);
+  const int nt = ((N >> 1) + kRT - 1) / kRT;  // tiles of the halved index
+  dim3 g(nt, nt, 2);
   int aFast = flw == 0 ? 1 : 0;
   if (c->precision == kC128)
     {
