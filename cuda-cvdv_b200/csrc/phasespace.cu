@@ -43,54 +43,69 @@ __device__ __forceinline__ uint64_t slice_addr(uint64_t o, uint64_t a, int flw, 
 
 // ----------------------------------------------------------------- rho GEMM
 constexpr int kRT = 64;   // output tile
-constexpr int kRK = 16;   // slices per k-step
+constexpr int kRK = 8;    // slices per k-step (two buffers of 2 x 8 x 65 complex: 33 KB)
 
 // The Wigner gather reads rho[a][b] only at a + b even (a = i - kd, b = i + kd), so
 // the GEMM forms the two same-parity blocks, a = 2 a' + par and b = 2 b' + par
 // (par = blockIdx.z), each an N/2 x N/2 Hermitian product: a quarter of the full
 // N x N x M work instead of half.  Tile indices below are in the halved index.
 template <typename C>
-__global__ void __launch_bounds__(256) k_rho(const C* __restrict__ st, int N, int q, int flw,
+__global__ void __launch_bounds__(256, 2) k_rho(const C* __restrict__ st, int N, int q, int flw,
                                             uint64_t M, double2* __restrict__ rho, int aFast) {
   int ta = blockIdx.y, tb = blockIdx.x;
   if (ta > tb) return;  // Hermitian: upper tiles only
-  __shared__ double2 sA[kRK][kRT + 1];
-  __shared__ double2 sB[kRK][kRT + 1];
+  // two operand buffers: the next k-step's slices are loaded into registers while
+  // the current one is multiplied, then stored to the other buffer (one barrier a step)
+  __shared__ double2 sA[2][kRK][kRT + 1];
+  __shared__ double2 sB[2][kRK][kRT + 1];
   const int par = blockIdx.z, Nh = N >> 1;
   const int a0 = ta * kRT, b0 = tb * kRT;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  constexpr int PER = kRK * kRT / 256;  // operand elements a thread loads per step
   double2 acc[4][4];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = make_double2(0.0, 0.0);
-  for (uint64_t o0 = 0; o0 < M; o0 += kRK) {
-    for (int e = threadIdx.x; e < kRK * kRT; e += 256) {
-      int kk, a;
-      if (aFast) {
-        a = e % kRT;
-        kk = e / kRT;
-      } else {
-        kk = e % kRK;
-        a = e / kRK;
-      }
-      uint64_t o = o0 + kk;
+  double2 ra[PER], rb[PER];
+  auto fetch = [&](uint64_t o0) {
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int e = threadIdx.x + 256 * u;
+      const int kk = aFast ? e / kRT : e % kRK, a = aFast ? e % kRT : e / kRK;
+      const uint64_t o = o0 + kk;
       double2 va = make_double2(0.0, 0.0), vb = make_double2(0.0, 0.0);
       if (o < M) {
         if (a0 + a < Nh) va = tod2<C>(st[slice_addr(o, 2 * (a0 + a) + par, flw, q)]);
         if (b0 + a < Nh) vb = tod2<C>(st[slice_addr(o, 2 * (b0 + a) + par, flw, q)]);
       }
-      sA[kk][a] = va;
-      sB[kk][a] = vb;
+      ra[u] = va;
+      rb[u] = vb;
     }
-    __syncthreads();
+  };
+  auto put = [&](int buf) {
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int e = threadIdx.x + 256 * u;
+      const int kk = aFast ? e / kRT : e % kRK, a = aFast ? e % kRT : e / kRK;
+      sA[buf][kk][a] = ra[u];
+      sB[buf][kk][a] = rb[u];
+    }
+  };
+  fetch(0);
+  put(0);
+  __syncthreads();
+  int buf = 0;
+  for (uint64_t o0 = 0; o0 < M; o0 += kRK) {
+    const bool more = o0 + kRK < M;
+    if (more) fetch(o0 + kRK);
 #pragma unroll 4
     for (int kk = 0; kk < kRK; ++kk) {
       double2 av[4], bv[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) av[i] = sA[kk][ty + 16 * i];
+      for (int i = 0; i < 4; ++i) av[i] = sA[buf][kk][ty + 16 * i];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) bv[j] = sB[kk][tx + 16 * j];
+      for (int j = 0; j < 4; ++j) bv[j] = sB[buf][kk][tx + 16 * j];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -100,7 +115,9 @@ __global__ void __launch_bounds__(256) k_rho(const C* __restrict__ st, int N, in
           acc[i][j].y += av[i].y * bv[j].x - av[i].x * bv[j].y;
         }
     }
+    if (more) put(buf ^ 1);  // that buffer was last read before the previous barrier
     __syncthreads();
+    buf ^= 1;
   }
 #pragma unroll
   for (int i = 0; i < 4; ++i)
