@@ -409,7 +409,7 @@ def _random_qubit_circuit(rng, qubits, n_gates):
 
 
 @pytest.mark.parametrize("qubits", [[1, 1, 1, 1, 1, 1, 8], [3, 2, 7], [1, 2, 1, 3, 1, 6], [2, 2, 2, 9],
-                                    [1, 2, 14]])
+                                    [1, 2, 14], [1, 1, 1, 1, 1, 1, 1, 7], [2, 1, 2, 2, 8]])
 def test_qubit_gate_sequences(qubits):
     """Chains of qubit gates run as qubit-gate sequence passes: equal to the oracle
     (plain and mixed) and to the per-gate pair path."""
