@@ -30,7 +30,8 @@ struct SeqTab {
 };
 
 struct SeqDiag {
-  double2 scalar;
+  double2 scalar;   // the run's constant factor where its dependent bit is 0
+  double2 scalar1;  // ... and where it is 1 (single-qubit phases folded in)
   int nTab;
   int g;  // selected-bit number (0..NB-1) the run depends on, or -1
   SeqTab tab[kSeqMaxTabs];
@@ -241,7 +242,7 @@ __global__ void __launch_bounds__(256, 2) k_seq(C* __restrict__ st, IDX nSites,
         }
       } else {
         const SeqDiag& D = P.diag[op.diag];
-        double2 w0 = D.scalar, w1 = D.scalar;
+        double2 w0 = D.scalar, w1 = D.scalar1;
         for (int t = 0; t < D.nTab; ++t) {
           const SeqTab& T = D.tab[t];
           int idx = (int)((base >> T.shift) & (IDX)T.mask);
@@ -383,15 +384,32 @@ bool launch_seq(Context* ctx, const std::vector<HostSeqOp>& ops) {
       set_error(ctx, kErrUnsupported, "qubit-gate sequence has too many diagonal runs");
       return false;
     }
+    // a phase on one selected qubit (Rz) is a pair of constants, g0 / g1 by that
+    // bit: fold it into the run's scalars instead of a two-entry table
+    std::vector<Term> rest;
+    double2 s0 = make_double2(1.0, 0.0), s1 = s0;
+    int foldBit = -1;
+    for (const Term& t : h.terms) {
+      const int gb = t.kind == kTermBit ? ctx->flw[t.r] + t.bit : -1;
+      if (gb >= 0 && std::find(bits.begin(), bits.end(), gb) != bits.end() && (foldBit < 0 || foldBit == gb)) {
+        foldBit = gb;
+        s0 = make_double2(s0.x * t.g0.x - s0.y * t.g0.y, s0.x * t.g0.y + s0.y * t.g0.x);
+        s1 = make_double2(s1.x * t.g1.x - s1.y * t.g1.y, s1.x * t.g1.y + s1.y * t.g1.x);
+        continue;
+      }
+      rest.push_back(t);
+    }
     FactorList F;
     std::vector<Term> left;
-    if (!build_factor_list(ctx, h.terms, &F, &left)) return false;
+    if (!build_factor_list(ctx, rest, &F, &left)) return false;
     if (!left.empty() || F.nXX || F.nTab > kSeqMaxTabs) {
       set_error(ctx, kErrUnsupported, "diagonal run does not fit a qubit-gate sequence");
       return false;
     }
     SeqDiag& D = P.diag[nd];
     D.scalar = F.hasScalar ? F.scalar : make_double2(1.0, 0.0);
+    D.scalar1 = make_double2(D.scalar.x * s1.x - D.scalar.y * s1.y, D.scalar.x * s1.y + D.scalar.y * s1.x);
+    D.scalar = make_double2(D.scalar.x * s0.x - D.scalar.y * s0.y, D.scalar.x * s0.y + D.scalar.y * s0.x);
     D.nTab = F.nTab;
     D.g = -1;
     for (int t = 0; t < F.nTab; ++t) {
@@ -417,6 +435,14 @@ bool launch_seq(Context* ctx, const std::vector<HostSeqOp>& ops) {
         S.d1 = d;
         D.g = b;
       }
+    }
+    if (foldBit >= 0) {
+      const int gi = (int)(std::find(bits.begin(), bits.end(), foldBit) - bits.begin());
+      if (D.g >= 0 && D.g != gi) {
+        set_error(ctx, kErrUnsupported, "diagonal run depends on two bits of a qubit-gate sequence");
+        return false;
+      }
+      D.g = gi;
     }
     o.kind = kSeqDiag;
     o.diag = nd++;
