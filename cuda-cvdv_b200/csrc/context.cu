@@ -281,6 +281,10 @@ bool build_factor_list(Context* ctx, const std::vector<Term>& terms, FactorList*
       T.mask = N - 1;
       T.ctrlShift = ctrl ? g.first.ctrl : -1;
       T.half = N;
+      // only controlled phases (Z = +-1 flips their sign): the halves are conjugate
+      T.conjHalf = ctrl ? 1 : 0;
+      for (size_t k = start; k < start + cnt && T.conjHalf; ++k)
+        T.conjHalf = ts[k].kind == kTermPoly && ts[k].ctrlBit == g.first.ctrl;
     }
   }
   for (const Term* t : xx) {

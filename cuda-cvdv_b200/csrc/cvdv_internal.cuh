@@ -84,6 +84,7 @@ struct TabFactor {
   int mask;       // N - 1
   int ctrlShift;  // global bit of a control qubit, -1 if none
   int half;       // N (offset of the ctrl=1 half)
+  int conjHalf;   // the ctrl=1 half is the complex conjugate of the ctrl=0 half
 };
 
 struct XXFactor {

@@ -25,8 +25,9 @@ namespace cvdv {
 struct SeqTab {
   const double2* ptr;
   int shift, mask, ctrlShift, half;
-  int dep;  // index depends on the run's selected bit
-  int d1;   // index offset when that bit is set
+  int dep;   // index depends on the run's selected bit
+  int d1;    // index offset when that bit is set
+  int conj;  // the entry at +d1 is the conjugate of the one at +0 (a controlled phase)
 };
 
 struct SeqDiag {
@@ -248,7 +249,7 @@ __global__ void __launch_bounds__(256, 2) k_seq(C* __restrict__ st, IDX nSites,
           int idx = (int)((base >> T.shift) & (IDX)T.mask);
           if (T.ctrlShift >= 0) idx += (int)((base >> T.ctrlShift) & (IDX)1) * T.half;
           const double2 a = __ldg(T.ptr + idx);
-          const double2 b = T.dep ? __ldg(T.ptr + idx + T.d1) : a;
+          const double2 b = T.dep ? (T.conj ? make_double2(a.x, -a.y) : __ldg(T.ptr + idx + T.d1)) : a;
           w0 = dmul(w0, a);
           w1 = dmul(w1, b);
         }
@@ -422,6 +423,7 @@ bool launch_seq(Context* ctx, const std::vector<HostSeqOp>& ops) {
       S.half = T.half;
       S.dep = 0;
       S.d1 = 0;
+      S.conj = 0;
       for (int b = 0; b < nb; ++b) {
         const uint64_t i = 1ull << bits[b];
         int d = (int)((i >> T.shift) & (uint64_t)T.mask);
@@ -433,6 +435,7 @@ bool launch_seq(Context* ctx, const std::vector<HostSeqOp>& ops) {
         }
         S.dep = 1;
         S.d1 = d;
+        S.conj = T.conjHalf && d == T.half;
         D.g = b;
       }
     }
