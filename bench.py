@@ -323,7 +323,7 @@ def run_gpu(args, world, rank, local):
     # scaled by the 16x larger state: the kernels stream the state once per launch,
     # so their traffic grows with the rows / sites processed.
     ncu_traffic_2p24 = {"fft_pass": ((269.3 + 219.8) + (269.1 + 222.2)) / 2 * 1e6,  # k_rowc, two launches
-                        "seq": (272.5 + 211.6) * 1e6}                                  # k_seq<double2, 5, 1, u32, 0>
+                        "seq": (270.4 + 212.4) * 1e6}                                  # k_seq<double2, 5, 1, u32, 0>
     scale = n_amp / float(1 << 24)
     traffic = ncu_traffic_2p24[dom] * scale if (dom in ncu_traffic_2p24 and args.workload == "full") else None
     achieved = kr[dom]["achieved_gbs"]
