@@ -16,7 +16,9 @@ to the final state and to the back-propagated target and reading
 forward states recovered by the inverse gates, not stored, and reset from a
 checkpoint every ``checkpoint_every`` gates to bound the drift.  Each step is
 one kernel over the whole batch (libcvdv ``cvdvBatch*``); there is no CPU
-fallback.
+fallback.  With ``graphs=True`` both sweeps are captured in CUDA graphs once per
+shape and replayed (the per-gate launch and Python overhead dominate at the
+configured sizes).
 
 The reference has no such form: its ``TorchCvdv`` casts gate parameters to
 Python scalars, so it cannot be differentiated.
@@ -46,8 +48,13 @@ def _check(code: int) -> None:
 
 class VariationalCircuit:
     def __init__(self, numQubits_list: Sequence[int], gates: Sequence[GateSpec],
-                 precision: str = "complex64", checkpoint_every: int = 16) -> None:
+                 precision: str = "complex64", checkpoint_every: int = 16, graphs: bool = False) -> None:
         self.qubits = list(numQubits_list)
+        # graphs=True: the forward sweep and the adjoint sweep are each captured once per
+        # (batch, psi0 shape, target shape) in a CUDA graph and replayed, on buffers
+        # owned by the circuit (one loss/backward pair at a time per shape)
+        self.graphs = bool(graphs)
+        self._plans = {}
         self.n = sum(self.qubits)
         self.mode = len(self.qubits) - 1
         self.precision = precision
@@ -130,7 +137,17 @@ class VariationalCircuit:
 
     def fidelity_loss(self, params: torch.Tensor, psi0: torch.Tensor, target: torch.Tensor) -> torch.Tensor:
         """1 - |<target|psi_b>|^2 for every instance b (float64, differentiable in params)."""
+        if self.graphs:
+            return _GraphFidelityLoss.apply(params, self, psi0, target)
         return _FidelityLoss.apply(params, self, psi0, target)
+
+    def _plan(self, B: int, psi0: torch.Tensor, target: torch.Tensor) -> "_GraphPlan":
+        key = (B, tuple(psi0.shape), tuple(target.shape))
+        plan = self._plans.get(key)
+        if plan is None:
+            plan = _GraphPlan(self, B, psi0.shape, target.shape)
+            self._plans[key] = plan
+        return plan
 
 
 class _FidelityLoss(torch.autograd.Function):
@@ -168,6 +185,91 @@ class _FidelityLoss(torch.autograd.Function):
                 psi.copy_(ck)
         gl = grad_loss.to(device=psi.device, dtype=torch.float64)
         return (grads.t() * gl[:, None]).to(ctx.params_device), None, None, None
+
+
+class _GraphPlan:
+    """Static buffers of one (batch, psi0, target) shape and the two captured
+    sweeps: forward (gates, checkpoints, overlap) and adjoint (gradients)."""
+
+    def __init__(self, circ: VariationalCircuit, B: int, psi0_shape, tgt_shape) -> None:
+        dev, cd = "cuda", circ.cdtype
+        self.circ = circ
+        self.p = torch.zeros(circ.n_gates, B, dtype=torch.float64, device=dev)
+        self.psi0 = torch.zeros(tuple(psi0_shape), dtype=cd, device=dev)
+        self.tgt = torch.zeros(tuple(tgt_shape), dtype=cd, device=dev)
+        self.psi = torch.empty(B, 1 << circ.n, dtype=cd, device=dev)
+        self.back = torch.empty_like(self.psi)
+        self.lam = torch.empty_like(self.psi)
+        self.ck = {g: torch.empty_like(self.psi)
+                   for g in range(circ.checkpoint_every, circ.n_gates, circ.checkpoint_every)}
+        self.grads = torch.empty(circ.n_gates, B, dtype=torch.float64, device=dev)
+        self.generation = 0
+        # one eager run of each sweep on a side stream (first-use set-up), then capture
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            self._forward()
+            self._backward()
+        torch.cuda.current_stream().wait_stream(side)
+        self.forward_graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.forward_graph):
+            self._forward()
+        self.backward_graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.backward_graph):
+            self._backward()
+
+    def _forward(self) -> None:
+        c = self.circ
+        self.psi.copy_(self.psi0.expand_as(self.psi))
+        for g in range(c.n_gates):
+            if g in self.ck:
+                self.ck[g].copy_(self.psi)  # the state before gate g
+            c._apply(self.psi, g, self.p[g])
+        self.ov = c._overlap(self.psi, self.tgt)
+
+    def _backward(self) -> None:
+        c = self.circ
+        self.back.copy_(self.psi)
+        self.lam.copy_(self.tgt.expand_as(self.lam))
+        for g in reversed(range(c.n_gates)):
+            gval = c._adjoint(self.back, self.lam, g, self.p[g])
+            self.grads[g] = 2.0 * (self.ov.conj() * gval).imag
+            ck = self.ck.get(g)
+            if ck is not None:
+                self.back.copy_(ck)
+
+
+class _GraphFidelityLoss(torch.autograd.Function):
+    """_FidelityLoss on captured sweeps: the same kernels in the same order."""
+
+    @staticmethod
+    def forward(ctx, params: torch.Tensor, circ: VariationalCircuit, psi0: torch.Tensor,
+                target: torch.Tensor) -> torch.Tensor:
+        if params.dim() != 2 or params.shape[1] != circ.n_gates:
+            raise ValueError(f"params must be (batch, {circ.n_gates})")
+        psi0 = psi0.to(device="cuda", dtype=circ.cdtype)
+        if psi0.shape[-1] != 1 << circ.n or psi0.dim() not in (1, 2):
+            raise ValueError(f"psi0 must be (2^{circ.n},) or (batch, 2^{circ.n})")
+        tgt = target.to(device="cuda", dtype=circ.cdtype)
+        plan = circ._plan(params.shape[0], psi0, tgt)
+        plan.p.copy_(params.detach().to(device="cuda", dtype=torch.float64).t())
+        plan.psi0.copy_(psi0)
+        plan.tgt.copy_(tgt)
+        plan.forward_graph.replay()
+        plan.generation += 1
+        ctx.plan, ctx.generation = plan, plan.generation
+        ctx.params_device = params.device
+        return (1.0 - plan.ov.abs() ** 2).to(params.device)
+
+    @staticmethod
+    def backward(ctx, grad_loss: torch.Tensor):
+        plan = ctx.plan
+        if plan.generation != ctx.generation:
+            raise RuntimeError("VariationalCircuit(graphs=True): another fidelity_loss of the same shape "
+                               "ran before this backward; run backward first or use graphs=False")
+        plan.backward_graph.replay()
+        gl = grad_loss.to(device="cuda", dtype=torch.float64)
+        return (plan.grads.t() * gl[:, None]).to(ctx.params_device), None, None, None
 
 
 def layered_gates(layers: int = 40) -> List[GateSpec]:

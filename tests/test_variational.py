@@ -137,3 +137,24 @@ def test_full_config_gradient_step():
         grads[precision] = p.grad.numpy()
     err = np.abs(grads["complex64"] - grads["complex128"]).max() / np.abs(grads["complex128"]).max()
     assert err < 1e-3, err
+
+
+def test_graph_replay_matches_eager():
+    """graphs=True (both sweeps captured once and replayed) gives the eager losses and
+    gradients, on two steps in a row with different parameters."""
+    from cvdv_b200.variational import VariationalCircuit, layered_gates
+    w, params, psi0, tgt = _problem(batch=8, layers=6, mode_qubits=9)
+    eager = VariationalCircuit([1, 9], layered_gates(6), precision="complex128", checkpoint_every=4)
+    graph = VariationalCircuit([1, 9], layered_gates(6), precision="complex128", checkpoint_every=4,
+                               graphs=True)
+    for step in range(2):
+        p = params.double() + 0.1 * step
+        out = []
+        for c in (eager, graph):
+            q = p.clone().requires_grad_(True)
+            loss = c.fidelity_loss(q, psi0, tgt)
+            loss.sum().backward()
+            out.append((loss.detach().cpu(), q.grad.detach().cpu()))
+        assert torch.allclose(out[0][0], out[1][0], rtol=0, atol=1e-12)
+        assert torch.allclose(out[0][1], out[1][1], rtol=0, atol=1e-10)
+
