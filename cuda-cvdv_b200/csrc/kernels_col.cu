@@ -5,8 +5,8 @@
 // amplitudes below it).  A "column" is one transform line: fixed outer and inner
 // indices, stride S along the register.  A CTA of 256 threads takes W adjacent
 // columns (adjacent inner indices, so every load and store instruction covers W
-// consecutive amplitudes) and keeps each column's L points in registers, 16 (or
-// 8) per thread; the Stockham stages of the row kernels (row_fft.cuh) exchange through
+// consecutive amplitudes) and keeps each column's L points in registers, 8 per
+// thread; the Stockham stages of the row kernels (row_fft.cuh) exchange through
 // one padded shared-memory line per column.  A pass runs a small program on its
 // columns: DFTs, diagonal runs (factor lists of the flat index) and the four-step
 // twiddle.
@@ -64,11 +64,10 @@ struct ColShape {
   static constexpr int HI = L >= 64 ? (L >> 6) : 1;
 };
 
-// points per thread of the column kernel (log2): 8 in complex128, so that three
-// CTAs fit an SM (24 warps instead of 16; 0.71 against 0.80 ms per pass of a
-// 2^26-amplitude state), 16 in complex64
-template <typename C> struct ColCE { static constexpr int v = 4; };
-template <> struct ColCE<double2> { static constexpr int v = 3; };
+// points per thread of the column kernel (log2): 8, so that three complex128 CTAs
+// (four complex64 ones) fit an SM instead of two -- 0.71 against 0.80 ms per
+// complex128 pass of a 2^26-amplitude state, 0.54 against 0.65 in complex64
+template <typename C> struct ColCE { static constexpr int v = 3; };
 
 // Pass shapes: the first half of a transform (diagonal runs on the loads, DFT,
 // four-step twiddle), a shared middle pass (DFT, runs, DFT, twiddle), the second
@@ -86,7 +85,7 @@ __device__ __forceinline__ void col_diags(C (&v)[1 << CE], const ColPass& P, uin
 }
 
 template <typename C, int LOGL, int KIND, int D1, int D2, int CE = ColCE<C>::v>
-__global__ void __launch_bounds__(kColThreads, CE >= 4 ? 2 : 3)
+__global__ void __launch_bounds__(kColThreads, CE >= 4 ? 2 : (sizeof(C) == sizeof(float2) ? 4 : 3))
     k_colr(const C* __restrict__ in, C* __restrict__ out, const __grid_constant__ ColPass P) {
   using S = ColShape<LOGL, CE>;
   constexpr int TPC = S::TPC, W = S::W, E = S::E;
