@@ -51,7 +51,14 @@ struct ColPass {
   const double2* tw;  // w_{2^logTwN}^e table of the context
   int nOps, nDiag;
   ColOp ops[kMaxColOps];
-  FactorList diag[kMaxColDiags];  // evaluated at input addresses before the first DFT, output ones after
+  // diagonal runs, evaluated at input addresses before the first DFT, output ones
+  // after: diag[d] per point, and the run's bilinear terms c x_reg x_other (control
+  // bit off the register) lin[d][0..nLin[d]) as a linear phase along the column
+  FactorList diag[kMaxColDiags];
+  int nLin[kMaxColDiags];
+  XXFactor lin[kMaxColDiags][kMaxXX];  // side 1: the other register
+  int logQ;            // register length 2^logQ
+  double regC, regDx;  // centre and spacing of the register's grid
 };
 
 // CE: log2 of the points a thread holds (16 or 8); the shared line of a column is
@@ -74,6 +81,40 @@ template <typename C> struct ColCE { static constexpr int v = 3; };
 // half (DFT, runs on the stores), or a whole run on a short register (the op list).
 enum ColKind : int { kColFirst = 0, kColMiddle = 1, kColLast = 2, kColWhole = 3 };
 
+// The linear phase of diagonal run d on the points t + TPC k (k < E) of a column
+// whose point m sits at b + m ax: a (j - regC) regDx at register index j = j0 + u m,
+// a = sum c x_other (sign by the control bit); two sincos, then a running product.
+template <typename C, int LOGL, int CE>
+__device__ __forceinline__ void col_lin(C (&v)[1 << CE], const ColPass& P, int d, uint64_t b, uint64_t ax,
+                                        int t) {
+  constexpr int TPC = ColShape<LOGL, CE>::TPC;
+  double a = 0.0;
+  for (int l = 0; l < P.nLin[d]; ++l) {
+    const XXFactor& X = P.lin[d][l];
+    const int j = (int)((b >> X.shift1) & (uint64_t)X.mask1);
+    double cc = X.coeff * (((double)j - X.c1) * X.dx1);
+    if (X.ctrlShift >= 0 && ((b >> X.ctrlShift) & 1ull)) cc = -cc;
+    a += cc;
+  }
+  a *= P.regDx;
+  const double j0 = (double)((b >> P.logS) & ((1ull << P.logQ) - 1));
+  const double u = (double)(ax >> P.logS);
+  double2 f, st;
+  sincos(a * (j0 + u * (double)t - P.regC), &f.y, &f.x);
+  sincos(a * u * (double)TPC, &st.y, &st.x);
+#pragma unroll
+  for (int k = 0; k < (1 << CE); ++k) {
+    v[k] = cmul(v[k], fromd<C>(f));
+    f = dmul(f, st);
+  }
+}
+
+template <typename C, int LOGL, int CE>
+__device__ __forceinline__ void col_lins(C (&v)[1 << CE], const ColPass& P, uint64_t b, uint64_t ax, int t) {
+  for (int d = 0; d < P.nDiag; ++d)
+    if (P.nLin[d]) col_lin<C, LOGL, CE>(v, P, d, b, ax, t);
+}
+
 template <typename C, int LOGL, int CE>
 __device__ __forceinline__ void col_diags(C (&v)[1 << CE], const ColPass& P, uint64_t b, uint64_t ax, int t) {
   constexpr int TPC = ColShape<LOGL, CE>::TPC;
@@ -81,6 +122,7 @@ __device__ __forceinline__ void col_diags(C (&v)[1 << CE], const ColPass& P, uin
 #pragma unroll
     for (int k = 0; k < (1 << CE); ++k)
       v[k] = cmul(v[k], fromd<C>(eval_factor(P.diag[d], b + (uint64_t)(t + TPC * k) * ax)));
+    if (P.nLin[d]) col_lin<C, LOGL, CE>(v, P, d, b, ax, t);
   }
 }
 
@@ -132,6 +174,7 @@ __global__ void __launch_bounds__(kColThreads, CE >= 4 ? 2 : (sizeof(C) == sizeo
     if constexpr (KIND == kColFirst)
       for (int d = 0; d < P.nDiag; ++d) v[k] = cmul(v[k], fromd<C>(eval_factor(P.diag[d], a)));
   }
+  if constexpr (KIND == kColFirst) col_lins<C, LOGL, CE>(v, P, bIn, P.axisIn, t);
   if constexpr (KIND == kColWhole) {
     // input and output addresses coincide (one pass over the whole register)
     for (int p = 0; p < P.nOps; ++p) {
@@ -144,6 +187,7 @@ __global__ void __launch_bounds__(kColThreads, CE >= 4 ? 2 : (sizeof(C) == sizeo
 #pragma unroll
         for (int k = 0; k < E; ++k)
           v[k] = cmul(v[k], fromd<C>(eval_factor(F, bOut + (uint64_t)(t + TPC * k) * P.axisOut)));
+        if (P.nLin[op.diag]) col_lin<C, LOGL, CE>(v, P, op.diag, bOut, P.axisOut, t);
       }
     }
   } else {
@@ -153,6 +197,7 @@ __global__ void __launch_bounds__(kColThreads, CE >= 4 ? 2 : (sizeof(C) == sizeo
       rr_stages<C, D2, LOGL, 0, CE>(v, smcol, t, loL, hiL);
     }
   }
+  if constexpr (KIND == kColLast) col_lins<C, LOGL, CE>(v, P, bOut, P.axisOut, t);
   constexpr int DT = KIND == kColMiddle ? D2 : D1;  // direction of the four-step twiddle
   const int nMask = (1 << P.logN) - 1;
 #pragma unroll
@@ -218,11 +263,45 @@ bool col_fft_ok(Context* ctx, int reg) {
   return q >= 4 && q <= 16 && logS >= 3 && ctx->totalQbt >= 12;
 }
 
+// A diagonal run of a column pass: the per-point factor list and the bilinear terms
+// applied as a linear phase.
+struct ColRun {
+  FactorList F;
+  int nLin = 0;
+  XXFactor lin[kMaxXX];
+};
+
+// The bilinear terms c x_reg x_other with the control bit off register reg (at most
+// kMaxXX) become linear phases; the rest goes to one factor list (false: it does not fit).
+static bool split_col_run(Context* ctx, int reg, const std::vector<Term>& terms, ColRun* R) {
+  const int lo = ctx->flw[reg], hi = lo + ctx->q[reg];
+  std::vector<Term> rest;
+  R->nLin = 0;
+  for (const Term& t : terms) {
+    const bool ctrlIn = t.ctrlBit >= lo && t.ctrlBit < hi;
+    if (t.kind != kTermXX || (t.r == reg) == (t.s == reg) || ctrlIn || R->nLin >= kMaxXX) {
+      rest.push_back(t);
+      continue;
+    }
+    const int o = t.r == reg ? t.s : t.r;
+    XXFactor& X = R->lin[R->nLin++];
+    X = XXFactor{};
+    X.shift1 = ctx->flw[o];
+    X.mask1 = (1 << ctx->q[o]) - 1;
+    X.c1 = (double)((1 << ctx->q[o]) - 1) * 0.5;
+    X.dx1 = ctx->dx[o];
+    X.coeff = t.coeff;
+    X.ctrlShift = t.ctrlBit;
+  }
+  std::vector<Term> left;
+  return build_factor_list(ctx, rest, &R->F, &left) && left.empty();
+}
+
 // A run of T >= 1 transforms (directions dirs) with the diagonal runs around
 // them: slots[0] before the first, slots[t] between transform t-1 and t,
 // slots[T] after the last (each slot a list of diagonal runs).
 static bool run_col_chain(Context* ctx, int reg, const std::vector<int>& dirs,
-                          const std::vector<std::vector<FactorList>>& slots) {
+                          const std::vector<std::vector<ColRun>>& slots) {
   const int q = ctx->q[reg], logS = ctx->flw[reg], n = ctx->totalQbt;
   const int T = (int)dirs.size();
   const uint64_t S = 1ull << logS, N = 1ull << q;
@@ -234,22 +313,27 @@ static bool run_col_chain(Context* ctx, int reg, const std::vector<int>& dirs,
     P.logTwN = logTwN;
     P.tw = ctx->twiddle;
     P.outerIn = P.outerOut = N * S;
+    P.logQ = q;
+    P.regC = (double)(N - 1) * 0.5;
+    P.regDx = ctx->dx[reg];
   };
-  auto add_op = [&](ColPass& P, int kind, int dir, const FactorList* F) -> bool {
+  auto add_op = [&](ColPass& P, int kind, int dir, const ColRun* F) -> bool {
     if (P.nOps >= kMaxColOps || (kind == kColDiag && P.nDiag >= kMaxColDiags)) return false;
     ColOp& op = P.ops[P.nOps++];
     op.kind = kind;
     op.dir = dir;
     op.diag = -1;
     if (kind == kColDiag) {
-      P.diag[P.nDiag] = *F;
+      P.diag[P.nDiag] = F->F;
+      P.nLin[P.nDiag] = F->nLin;
+      for (int l = 0; l < F->nLin; ++l) P.lin[P.nDiag][l] = F->lin[l];
       op.diag = P.nDiag++;
     }
     return true;
   };
   auto add_slot = [&](ColPass& P, int s) -> bool {
-    for (const FactorList& F : slots[s])
-      if (!factor_empty(F) && !add_op(P, kColDiag, 0, &F)) return false;
+    for (const ColRun& F : slots[s])
+      if ((!factor_empty(F.F) || F.nLin) && !add_op(P, kColDiag, 0, &F)) return false;
     return true;
   };
   auto go = [&](const ColPass& P, int logL, int kind, int d1, int d2) -> bool {
@@ -308,7 +392,10 @@ static bool run_col_chain(Context* ctx, int reg, const std::vector<int>& dirs,
 }
 
 bool launch_col_fft(Context* ctx, int reg, int dir, const FactorList& pre, const FactorList& post) {
-  return run_col_chain(ctx, reg, {dir}, {{pre}, {post}});
+  ColRun a, b;
+  a.F = pre;
+  b.F = post;
+  return run_col_chain(ctx, reg, {dir}, {{a}, {b}});
 }
 
 // A row-program style run (transforms of `reg` and diagonal runs, in order) on a
@@ -316,21 +403,19 @@ bool launch_col_fft(Context* ctx, int reg, int dir, const FactorList& pre, const
 // passes for longer ones.
 bool launch_col_chain(Context* ctx, int reg, const std::vector<HostRowOp>& ops) {
   std::vector<int> dirs;
-  std::vector<std::vector<FactorList>> slots(1);
+  std::vector<std::vector<ColRun>> slots(1);
   for (const HostRowOp& h : ops) {
     if (h.kind == kRowFft) {
       dirs.push_back(h.dir);
       slots.emplace_back();
       continue;
     }
-    FactorList F;
-    std::vector<Term> left;
-    if (!build_factor_list(ctx, h.terms, &F, &left)) return false;
-    if (!left.empty()) {
+    ColRun R;
+    if (!split_col_run(ctx, reg, h.terms, &R)) {
       set_error(ctx, kErrUnsupported, "column transform run: diagonal run does not fit");
       return false;
     }
-    slots.back().push_back(F);
+    slots.back().push_back(R);
   }
   if (dirs.empty()) {
     set_error(ctx, kErrUnsupported, "column transform run without a transform");
