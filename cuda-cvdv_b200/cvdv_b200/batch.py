@@ -270,9 +270,19 @@ class BatchedCircuits:
         self._progs = torch.from_numpy(prog_arr.view(np.uint8).copy()).cuda()
         self._tasks = []
         for tl in stage_tasks:
+            # the CTAs take tasks round-robin: largest first, so the long row programs
+            # start in the first wave instead of trailing the stage
+            tl = sorted(tl, key=self._task_cost, reverse=True)
             arr = np.array(tl, dtype=TASK_DTYPE) if tl else np.zeros(0, dtype=TASK_DTYPE)
             self._validate(arr)
             self._tasks.append((torch.from_numpy(arr.view(np.uint8).copy()).cuda(), len(arr)))
+
+    @staticmethod
+    def _task_cost(t: np.void) -> int:
+        """Amplitudes a task touches, row programs weighted for their transforms."""
+        if int(t["kind"]) == 0:
+            return (int(t["count"]) << int(t["logRow"])) * 4
+        return int(t["count"]) * 2
 
     def _row_tasks(self, i: int, n: int, m: int, prog: int, per: int) -> List[np.void]:
         out = []
