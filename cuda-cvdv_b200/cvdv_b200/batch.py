@@ -268,21 +268,23 @@ class BatchedCircuits:
         self.n_programs = len(progs)
         prog_arr = np.array(progs, dtype=PROGRAM_DTYPE) if progs else np.zeros(1, dtype=PROGRAM_DTYPE)
         self._progs = torch.from_numpy(prog_arr.view(np.uint8).copy()).cuda()
+        nfft = [int(np.isin(pr["op"][: pr["nOps"]], (OP_FWD, OP_INV)).sum()) for pr in progs]
+
+        def cost(t: np.void) -> int:
+            """Work of a task: amplitudes, times the transforms' log2 length for row programs."""
+            if int(t["kind"]) == 0:
+                m = int(t["logRow"])
+                return (int(t["count"]) << m) * (2 + nfft[int(t["program"])] * m)
+            return int(t["count"]) * 4
+
         self._tasks = []
         for tl in stage_tasks:
             # the CTAs take tasks round-robin: largest first, so the long row programs
             # start in the first wave instead of trailing the stage
-            tl = sorted(tl, key=self._task_cost, reverse=True)
+            tl = sorted(tl, key=cost, reverse=True)
             arr = np.array(tl, dtype=TASK_DTYPE) if tl else np.zeros(0, dtype=TASK_DTYPE)
             self._validate(arr)
             self._tasks.append((torch.from_numpy(arr.view(np.uint8).copy()).cuda(), len(arr)))
-
-    @staticmethod
-    def _task_cost(t: np.void) -> int:
-        """Amplitudes a task touches, row programs weighted for their transforms."""
-        if int(t["kind"]) == 0:
-            return (int(t["count"]) << int(t["logRow"])) * 4
-        return int(t["count"]) * 2
 
     def _row_tasks(self, i: int, n: int, m: int, prog: int, per: int) -> List[np.void]:
         out = []
