@@ -256,8 +256,8 @@ static cudaError_t col_dispatch(Context* ctx, int logL, const ColPass& P, int ki
 
 // Whether the column kernel takes transforms of register `reg`: 2^4..2^16 points
 // and at least 8 amplitudes below it (runs of 8 contiguous columns for the loads
-// and stores).  A pass of 2^l points has 2^(n-l) columns and 2^(12-l) columns per
-// CTA, so n >= 12 fills every CTA.
+// and stores).  A pass of 2^l points has 2^(n-l) columns and 2^(11-l) columns per
+// CTA (8 points a thread), so n >= 12 fills every CTA.
 bool col_fft_ok(Context* ctx, int reg) {
   const int q = ctx->q[reg], logS = ctx->flw[reg];
   return q >= 4 && q <= 16 && logS >= 3 && ctx->totalQbt >= 12;
