@@ -236,7 +236,7 @@ def run_reference(args, world, rank):
                    "step": "one gate of the circuit (cycling), CPU oracle"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{len(timed)} gates of the {len(circ['gates'])}-gate circuit at 2^{n_tot} "
-                                   f"(numpy elementwise single-threaded, scipy FFT on {threads} threads)"},
+                                   f"(numpy elementwise slabs and scipy FFT on {threads} threads)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

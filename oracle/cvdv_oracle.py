@@ -53,6 +53,28 @@ except ImportError:  # pragma: no cover
 PI = 3.14159265358979323846
 SQRT2 = 1.41421356237309504880
 
+_POOLS: dict = {}
+
+
+def _pool(workers: int):
+    """Shared thread pool for the elementwise passes (numpy releases the GIL
+    inside its loops, so chunks of one multiply run on separate cores)."""
+    if workers <= 1:
+        return None
+    if workers not in _POOLS:
+        from concurrent.futures import ThreadPoolExecutor
+        _POOLS[workers] = ThreadPoolExecutor(max_workers=workers)
+    return _POOLS[workers]
+
+
+def _ranges(n: int, parts: int):
+    step = -(-n // parts)
+    return [(a, min(a + step, n)) for a in range(0, n, step)]
+
+
+# states smaller than this stay on the single-threaded numpy path
+_THREAD_MIN = 1 << 20
+
 
 def c_round(x: float) -> float:
     """C ``round()``: halves away from zero (used by ``gates.cu:470,514``)."""
@@ -91,6 +113,32 @@ class OracleCvdv:
         shape[axis] = -1
         return vec.reshape(shape)
 
+    def _mul(self, fac) -> None:
+        """``state *= fac`` with ``fac`` broadcastable to the register-indexed
+        shape.  With ``workers > 1`` the state is cut into slabs along its
+        leading registers and the slabs are multiplied in place on a thread
+        pool; elementwise, so every amplitude gets the same product."""
+        fac = np.asarray(fac)
+        fac = fac.reshape((1,) * (self.R - fac.ndim) + fac.shape)
+        pool = _pool(self.workers)
+        if pool is None or self.size < _THREAD_MIN:
+            self.state = (self._t() * fac).reshape(-1)
+            return
+        s, P = 0, 1
+        while s < self.R and P < 16 * self.workers:
+            P *= self.dims[s]
+            s += 1
+        st = np.ascontiguousarray(self.state)
+        tv = st.reshape((P,) + tuple(self.dims[s:]))
+        fv = np.broadcast_to(fac, tuple(self.dims[:s]) + fac.shape[s:]).reshape((P,) + fac.shape[s:])
+
+        def run(ab):
+            a, b = ab
+            np.multiply(tv[a:b], fv[a:b], out=tv[a:b])
+
+        list(pool.map(run, _ranges(P, 4 * self.workers)))
+        self.state = st
+
     def _ctrl_sign(self, ctrl_reg: int, ctrl_qubit: int) -> np.ndarray:
         """+1 where the control qubit is 0, -1 where it is 1 (``gates.cuh:31-37``)."""
         Nc = self.dims[ctrl_reg]
@@ -102,7 +150,7 @@ class OracleCvdv:
         """Multiply by exp(i*phase(j_a, j_b)); handles reg_a == reg_b."""
         if reg_a == reg_b:
             ph = phase_fn(np.arange(self.dims[reg_a]), np.arange(self.dims[reg_a]), diag=True)
-            self.state = (self._t() * self._bcast(np.exp(1j * ph), reg_a)).reshape(-1)
+            self._mul(self._bcast(np.exp(1j * ph), reg_a))
             return
         ja = np.arange(self.dims[reg_a])[:, None]
         jb = np.arange(self.dims[reg_b])[None, :]
@@ -113,7 +161,7 @@ class OracleCvdv:
         shape[reg_b] = self.dims[reg_b]
         if reg_a > reg_b:
             fac = fac.T
-        self.state = (self._t() * fac.reshape(shape)).reshape(-1)
+        self._mul(fac.reshape(shape))
 
     # ------------------------------------------------------------ init / io
     def init_from_separable(self, arrays: Sequence[np.ndarray]) -> None:
@@ -140,7 +188,7 @@ class OracleCvdv:
     def phase_x(self, r: int, c: float) -> None:
         """``kernelPhaseX`` (``gates.cuh:5-16``): psi *= exp(i c x)."""
         ph = c * self.grid(r)
-        self.state = (self._t() * self._bcast(np.exp(1j * ph), r)).reshape(-1)
+        self._mul(self._bcast(np.exp(1j * ph), r))
 
     def cphase_x(self, t: int, cr: int, cq: int, c: float) -> None:
         """``kernelCPhaseX`` (``gates.cuh:20-38``): exp(i c Z x)."""
@@ -153,7 +201,7 @@ class OracleCvdv:
     def phase_x2(self, r: int, tcoef: float) -> None:
         """``kernelPhaseX2`` (``gates.cuh:184-196``): exp(i t x^2)."""
         x = self.grid(r)
-        self.state = (self._t() * self._bcast(np.exp(1j * (tcoef * x * x)), r)).reshape(-1)
+        self._mul(self._bcast(np.exp(1j * (tcoef * x * x)), r))
 
     def cphase_x2(self, t: int, cr: int, cq: int, tcoef: float) -> None:
         """``kernelCPhaseX2`` (``gates.cuh:42-60``): exp(i t Z x^2)."""
@@ -167,7 +215,7 @@ class OracleCvdv:
     def phase_x3(self, r: int, c: float) -> None:
         """``kernelPhaseX3`` (``gates.cuh:198-209``): exp(i c x^3)."""
         x = self.grid(r)
-        self.state = (self._t() * self._bcast(np.exp(1j * (c * x * x * x)), r)).reshape(-1)
+        self._mul(self._bcast(np.exp(1j * (c * x * x * x)), r))
 
     def phase_xx(self, r1: int, r2: int, c: float) -> None:
         """``kernelPhaseXX`` (``gates.cuh:213-231``): exp(i c x1 x2)."""
@@ -186,11 +234,11 @@ class OracleCvdv:
 
     def global_scalar(self, s: float) -> None:
         """``kernelGlobalScalar`` (``gates.cuh:262-268``)."""
-        self.state = self.state * s
+        self._mul(np.float64(s))
 
     def global_phase(self, phi: float) -> None:
         """``kernelGlobalPhase`` (``gates.cuh:271-275``)."""
-        self.state = self.state * np.exp(1j * phi)
+        self._mul(np.exp(1j * phi))
 
     # ------------------------------------------------------------ basis change
     def ft_q2p(self, r: int) -> None:
@@ -217,6 +265,10 @@ class OracleCvdv:
     def _pair(self, r: int, k: int, m00, m01, m10, m11) -> None:
         """2x2 update on the pairs differing in one bit (``utils.cuh:79-84``)."""
         b = self.flw[r] + self.q[r] - 1 - k
+        pool = _pool(self.workers)
+        if pool is not None and self.size >= _THREAD_MIN:
+            self._pair_threaded(pool, b, m00, m01, m10, m11)
+            return
         v = self.state.reshape(-1, 2, 1 << b)
         a0 = v[:, 0, :].copy()
         a1 = v[:, 1, :].copy()
@@ -224,6 +276,24 @@ class OracleCvdv:
         out[:, 0, :] = m00 * a0 + m01 * a1
         out[:, 1, :] = m10 * a0 + m11 * a1
         self.state = out.reshape(-1)
+
+    def _pair_threaded(self, pool, b: int, m00, m01, m10, m11) -> None:
+        """``_pair`` in place, slabs of pairs on the thread pool."""
+        st = np.ascontiguousarray(self.state)
+        v = st.reshape(-1, 2, 1 << b)
+        A, B = v.shape[0], v.shape[2]
+        parts = 4 * self.workers
+
+        def run(ab):
+            a, e = ab
+            sl = (slice(a, e), slice(None)) if A >= parts else (slice(None), slice(a, e))
+            a0 = v[sl[0], 0, sl[1]].copy()
+            a1 = v[sl[0], 1, sl[1]]
+            v[sl[0], 0, sl[1]] = m00 * a0 + m01 * a1
+            v[sl[0], 1, sl[1]] = m10 * a0 + m11 * a1
+
+        list(pool.map(run, _ranges(A if A >= parts else B, parts)))
+        self.state = st
 
     def pauli_rotation(self, r: int, k: int, axis: int, theta: float) -> None:
         """``kernelPauliRotation`` (``gates.cuh:63-92``)."""

@@ -240,3 +240,23 @@ def test_coherent_restatement_matches_reference_setter():
     """The helper above equals the reference SeparableState.setCoherent output."""
     for a in (1.0, 1.5 + 0.8j, -0.5 + 2.0j):
         np.testing.assert_allclose(_coherent(6, complex(a)), SEP[f"coherent_6_{a}"], atol=1e-15)
+
+
+def test_threaded_passes_match_single_threaded():
+    """The CPU timing arm runs the oracle with a thread pool over slabs of the
+    state; the slabs must give the same amplitudes as the one-thread path."""
+    from oracle.cvdv_oracle import OracleSim
+    rng = np.random.default_rng(11)
+    qubits = [1, 2, 1, 2, 14]
+    n = sum(qubits)
+    psi = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    gates = [("h", (0, 0)), ("cd", (4, 1, 1, 0.4 - 0.2j)), ("rz", (3, 1, 0.7)), ("rx", (2, 0, 0.3)),
+             ("d", (4, 0.3 + 0.1j)), ("r", (4, 0.5)), ("s", (4, 0.2)), ("h", (4, 0)), ("h", (4, 13)),
+             ("cr", (4, 0, 0, 0.25)), ("p", (4,))]
+    sims = [OracleSim(qubits, workers=w) for w in (1, 3)]
+    for o in sims:
+        o.set_state(psi)
+        for meth, args in gates:
+            getattr(o, meth)(*args)
+    a, b = sims[0].get_state(), sims[1].get_state()
+    assert np.max(np.abs(a - b)) <= 1e-12 * np.max(np.abs(a))
