@@ -327,8 +327,49 @@ CVDVContext* cvdvCreate(int numReg, int* numQubits) {
   return cvdvCreateEx(numReg, numQubits, kC128);
 }
 
+}  // extern "C"
+
+namespace cvdv {
+
+Context* factor_context(Context* ctx, int r) {
+  if ((int)ctx->factorCtx.size() < ctx->numReg) ctx->factorCtx.resize(ctx->numReg, nullptr);
+  if (ctx->factorCtx[r]) return ctx->factorCtx[r];
+  int q = ctx->q[r];
+  CVDVContext* h = cvdvCreateEx(1, &q, kC128);
+  if (!h) {
+    set_error(ctx, kErrAlloc, "register %d context: out of host memory", r);
+    return nullptr;
+  }
+  Context* f = h;
+  if (f->numReg != 1) {
+    set_error(ctx, f->lastErr != kOk ? f->lastErr : kErrAlloc, "register %d context: %s", r,
+              f->lastMsg.c_str());
+    cvdvDestroy(h);
+    return nullptr;
+  }
+  cudaStreamSynchronize(f->stream);  // its twiddle table
+  cudaStreamDestroy(f->stream);
+  f->stream = ctx->stream;  // stream order keeps its kernels between this context's
+  ctx->factorCtx[r] = f;
+  return f;
+}
+
+}  // namespace cvdv
+
+extern "C" {
+
 static void release(Context* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
+  for (Context* f : c->factorCtx)
+    if (f) {
+      f->stream = nullptr;  // this context's stream, destroyed with it
+      cvdvDestroy(static_cast<CVDVContext*>(f));
+    }
+  c->factorCtx.clear();
+  if (c->factors) cudaFree(c->factors);
+  c->factors = nullptr;
+  c->factorsCap = 0;
+  c->productPending = false;
   for (int k = 0; k < 2; ++k) {
     if (c->buf[k]) cudaFree(c->buf[k]);
     c->buf[k] = nullptr;
@@ -389,10 +430,38 @@ void cvdvInitFromSeparable(CVDVContext* ctx, void** devicePtrs, int numReg) {
       return;
     }
   c->pending.clear();  // a new state replaces whatever the queued gates would have produced
+  c->productPending = false;
   if (!ensure_state(c)) return;
-  arena_reset(c);
   size_t totalN = 0;
   for (int r = 0; r < numReg; ++r) totalN += (size_t)1 << c->q[r];
+  if (c->deferProduct && numReg >= 2) {
+    // keep the arrays; the next flush forms the product (context.cu, form_product)
+    if (c->factorsCap < totalN) {
+      if (c->factors) cudaFree(c->factors);
+      c->factors = nullptr;
+      c->factorsCap = 0;
+      if (cudaMalloc((void**)&c->factors, totalN * sizeof(double2)) != cudaSuccess) {
+        cudaGetLastError();
+        set_error(c, kErrAlloc, "cvdvInitFromSeparable: register arrays (%zu bytes)",
+                  totalN * sizeof(double2));
+        return;
+      }
+      c->factorsCap = totalN;
+    }
+    size_t off = 0;
+    for (int r = 0; r < numReg; ++r) {
+      size_t N = (size_t)1 << c->q[r];
+      if (!cuda_ok(c, cudaMemcpyAsync(c->factors + off, devicePtrs[r], N * sizeof(double2),
+                                      cudaMemcpyDefault, c->stream),
+                   "cvdvInitFromSeparable copy"))
+        return;
+      off += N;
+    }
+    c->productPending = true;
+    c->initialized = true;
+    return;
+  }
+  arena_reset(c);
   double2* base = (double2*)arena_alloc(c, totalN * sizeof(double2));
   if (!base) return;
   std::vector<const double2*> arrs(numReg);
@@ -418,6 +487,7 @@ void cvdvSetStateFromDevicePtr(CVDVContext* ctx, void* d_src) {
   if (!ctx || !d_src) return;
   Context* c = C(ctx);
   c->pending.clear();
+  c->productPending = false;
   if (!ensure_state(c)) return;
   uint64_t n = c->size();
   if (c->precision == kC128) {
@@ -498,6 +568,7 @@ void cvdvSetFusion(CVDVContext* ctx, int flags) {
   C(ctx)->fuseSeq = (flags & 2) != 0;
   C(ctx)->colFft = (flags & 4) != 0;
   C(ctx)->colProg = (flags & 8) != 0;
+  C(ctx)->deferProduct = (flags & 16) != 0;
 }
 
 long long cvdvCancelledTransforms(CVDVContext* ctx) { return ctx ? C(ctx)->ftCancelled * 2 : 0; }

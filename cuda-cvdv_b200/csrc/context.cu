@@ -514,8 +514,100 @@ static bool stage_commutes(Context* ctx, const Stage& y, const Stage& x) {
   }
 }
 
+// Product deferral.  After cvdvInitFromSeparable the state is the product of the
+// register arrays.  A stage that acts on register r alone, queued ahead of every
+// stage that couples r to another register, commutes with the stages before it
+// (they act on other registers or on r alone), so it can run on r's array before
+// the product is formed.  Such stages of registers of kFactorMinQ..kFactorMaxQ
+// qubits run, in queue order, in a one-register complex128 context on this
+// context's stream; qubit registers keep theirs (they join the qubit-gate
+// sequences).  Stages that stay are left in order; the product is formed from
+// the updated arrays.
+constexpr int kFactorMinQ = 8, kFactorMaxQ = 14;
+
+static Stage factor_stage(Context* ctx, Stage s, int r) {
+  const int f = ctx->flw[r];
+  switch (s.kind) {
+    case kStFft: s.reg = 0; break;
+    case kStPair: s.bit -= f; break;
+    case kStPerm:
+      s.reg = 0;
+      if (s.reg2 >= 0) s.reg2 = 0;
+      if (s.bit >= 0) s.bit -= f;
+      break;
+    default:
+      for (Term& t : s.terms) {
+        if (t.kind == kTermScalar) continue;
+        t.r = 0;
+        if (t.kind == kTermXX) t.s = 0;
+        if (t.ctrlBit >= 0) t.ctrlBit -= f;
+      }
+  }
+  if (s.ftTag) s.ftReg = 0;
+  return s;
+}
+
+static bool form_product(Context* ctx, std::vector<Stage>& stages) {
+  const int R = ctx->numReg;
+  std::vector<std::vector<Stage>> per(R);
+  std::vector<char> coupled(R, 0);
+  std::vector<Stage> rest;
+  rest.reserve(stages.size());
+  for (Stage& s : stages) {
+    int reg = -1, n = 0;
+    for (int r = 0; r < R; ++r)
+      if (stage_touches_reg(ctx, s, r)) {
+        reg = r;
+        ++n;
+      }
+    if (n == 1 && !coupled[reg] && ctx->q[reg] >= kFactorMinQ && ctx->q[reg] <= kFactorMaxQ) {
+      per[reg].push_back(factor_stage(ctx, std::move(s), reg));
+      continue;
+    }
+    if (n > 1)
+      for (int r = 0; r < R; ++r)
+        if (stage_touches_reg(ctx, s, r)) coupled[r] = 1;
+    rest.push_back(std::move(s));
+  }
+  std::vector<const double2*> arrs(R);
+  size_t off = 0;
+  for (int r = 0; r < R; ++r) {
+    arrs[r] = ctx->factors + off;
+    off += (size_t)1 << ctx->q[r];
+  }
+  for (int r = 0; r < R; ++r) {
+    if (per[r].empty()) continue;
+    Context* f = factor_context(ctx, r);
+    if (!f) return false;
+    const size_t bytes = ((size_t)1 << ctx->q[r]) * sizeof(double2);
+    bool ok = ensure_state(f) &&
+              cuda_ok(f, cudaMemcpyAsync(f->state(), arrs[r], bytes, cudaMemcpyDeviceToDevice, f->stream),
+                      "register array in");
+    if (ok) {
+      f->initialized = true;
+      f->cancelFt = ctx->cancelFt;
+      f->fuseSeq = ctx->fuseSeq;
+      f->colFft = ctx->colFft;
+      f->colProg = ctx->colProg;
+      f->pending = std::move(per[r]);
+      ok = flush(f) && cuda_ok(f, cudaMemcpyAsync((void*)arrs[r], f->state(), bytes,
+                                                   cudaMemcpyDeviceToDevice, f->stream),
+                               "register array out");
+    }
+    if (!ok) {
+      set_error(ctx, f->lastErr != kOk ? f->lastErr : kErrCuda, "register %d before the product: %s", r,
+                f->lastMsg.c_str());
+      return false;
+    }
+  }
+  if (!launch_init_product(ctx, arrs.data())) return false;
+  ctx->productPending = false;
+  stages.swap(rest);
+  return true;
+}
+
 bool flush(Context* ctx) {
-  if (ctx->pending.empty()) return true;
+  if (ctx->pending.empty() && !ctx->productPending) return true;
   if (!ctx->initialized) {
     set_error(ctx, kErrNotInitialized, "gates queued before the state was initialised");
     ctx->pending.clear();
@@ -524,6 +616,15 @@ bool flush(Context* ctx) {
   arena_reset(ctx);
   std::vector<Stage> stages;
   stages.swap(ctx->pending);
+  if (ctx->productPending) {
+    if (!form_product(ctx, stages)) {
+      // the state is lost with the product: later calls report it uninitialised
+      ctx->productPending = false;
+      ctx->initialized = false;
+      return false;
+    }
+    if (stages.empty()) return true;
+  }
   if (ctx->fuseSeq) hoist_pairs_past_transforms(ctx, stages);
   std::vector<Op> ops;
   std::vector<Term> diag;

@@ -264,6 +264,15 @@ struct Context {
   bool fuseSeq = true;  // run chains of qubit gates as one qubit-gate sequence pass
   bool colFft = true;   // transforms of strided registers by the register-resident column kernel
   bool colProg = true;  // programs on strided registers by the register-resident row kernel in column form
+  // Product deferral (on by default, cvdvSetFusion bit 4): cvdvInitFromSeparable
+  // keeps the register arrays and the next flush forms the product, after the
+  // queued stages that act on one register alone, ahead of every stage that
+  // couples it to another register, have run on that register's array.
+  bool deferProduct = true;
+  bool productPending = false;
+  double2* factors = nullptr;       // the register arrays, concatenated (complex128)
+  size_t factorsCap = 0;            // in elements
+  std::vector<Context*> factorCtx;  // one-register contexts for them, made on first use
   // Inside one flush, between a forward and an inverse 2^14-point transform of
   // the last register run by the two-CTA row kernel, that register may be stored
   // "blocked": position r M + k2 holds logical index r + 2 k2 (the transform's
@@ -301,6 +310,8 @@ void arena_reset(Context* ctx);
 void* big_scratch(Context* ctx, size_t bytes);   // persistent, grown on demand
 double* host_scratch(Context* ctx, size_t count);
 bool ensure_state(Context* ctx);                  // allocate both buffers
+// complex128 context of the one register r of ctx, on ctx's stream (api_gates.cu)
+Context* factor_context(Context* ctx, int r);
 bool flush(Context* ctx);                         // run pending stages
 
 // planner/launch helpers (plan.cu)

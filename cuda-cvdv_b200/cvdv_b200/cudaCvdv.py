@@ -58,9 +58,11 @@ class CudaCvdv:
         identity); bit 1 runs chains of qubit gates on up to five qubits as one
         pass; bit 2 transforms non-last registers with the register-resident
         column kernel; bit 3 runs transform/diagonal runs on a non-last register
-        as one pass with each column on chip.  True = all, False = none, an int
-        = those bits."""
-        flags = (15 if on else 0) if isinstance(on, bool) else int(on)
+        as one pass with each column on chip; bit 4 applies the gates queued
+        after initStateVector that act on one mode alone (before it is coupled
+        to another register) to that mode's array before the product state is
+        formed.  True = all, False = none, an int = those bits."""
+        flags = (31 if on else 0) if isinstance(on, bool) else int(on)
         self._L.cvdvSetFusion(self.ctx, flags)
 
     def __del__(self):

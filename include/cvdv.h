@@ -48,7 +48,9 @@ void cvdvDestroy(CVDVContext* ctx);
 void cvdvFree(CVDVContext* ctx);
 /* src/cuda/context.cu:75-115 (api.h:17).  devicePtrs[r] points to N_r
  * complex128 values (device or host memory); psi = tensor product, last
- * register fastest, not normalised.  Built on the device. */
+ * register fastest, not normalised.  Built on the device, at the next flush
+ * (cvdvSetFusion bit 4).  The arrays are copied on the context's stream, so the
+ * caller's buffers must stay valid until that stream has run (cvdvSynchronize). */
 void cvdvInitFromSeparable(CVDVContext* ctx, void** devicePtrs, int numReg);
 /* src/cuda/context.cu:131-137 (api.h:18).  d_src: 2^n complex128 values
  * (device or host memory). */
@@ -164,8 +166,12 @@ void* cvdvGetStream(CVDVContext* ctx);
  * column DFTs (one pass up to 2^8 points, two passes up to 2^16) instead of the
  * shared-memory tile passes.  flags bit 3 (default on): a run of transforms and
  * diagonal gates on such a register (2^8 .. 2^13 points, 2^14 in complex64) runs
- * as one pass with each column held on chip.  cvdvCancelledTransforms
- * counts the transforms removed so far. */
+ * as one pass with each column held on chip.  flags bit 4 (default on): after
+ * cvdvInitFromSeparable on two or more registers, the queued stages that act on
+ * one register of 2^8 .. 2^14 points alone, ahead of every stage that couples it
+ * to another register, run on that register's array before the product is formed
+ * (at the next flush).  cvdvCancelledTransforms counts the transforms removed so
+ * far. */
 void cvdvSetFusion(CVDVContext* ctx, int flags);
 long long cvdvCancelledTransforms(CVDVContext* ctx);
 /* Number of kernels this library has launched in the process so far. */

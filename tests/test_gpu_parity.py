@@ -594,3 +594,98 @@ def test_full_size_state_transfer_properties():
     after = sim.stateTensor()
     err = float(torch.linalg.vector_norm(after - before) / torch.linalg.vector_norm(before))
     assert err < 1e-12
+
+
+def _separable(qubits, rng):
+    from cvdv_b200 import SeparableState
+    sep = SeparableState(list(qubits))
+    for r, q in enumerate(qubits):
+        a = rng.standard_normal(1 << q) + 1j * rng.standard_normal(1 << q)
+        sep.setCoeffs(r, torch.from_numpy(a / np.linalg.norm(a)))
+    return sep
+
+
+def _deferral_circuit(qubits, rng, couple_modes):
+    """Single-mode gates of every kind on each mode, qubit gates, then gates that
+    couple registers, then more single-mode gates."""
+    modes = [r for r, q in enumerate(qubits) if q >= 8]
+    qregs = [r for r, q in enumerate(qubits) if q < 8]
+    seq = []
+    for m in modes:
+        seq += [("s", (m, 0.3)), ("d", (m, complex(rng.normal(0, 0.5), rng.normal(0, 0.5)))), ("r", (m, 0.7)),
+                ("sheer", (m, 0.05)), ("phaseCubic", (m, 0.01)), ("h", (m, 1)), ("p", (m,)), ("ftQ2P", (m,))]
+    for qr in qregs:
+        seq.append(("h", (qr, 0)))
+    if qregs:
+        seq.append(("cd", (modes[0], qregs[0], 0, 0.4 + 0.1j)))
+    if couple_modes and len(modes) > 1:
+        seq.append(("bs", (modes[0], modes[1], 0.3)))
+    for m in modes:
+        seq += [("d", (m, 0.2 - 0.3j)), ("ftP2Q", (m,)), ("r", (m, -0.4))]
+    return seq
+
+
+@pytest.mark.parametrize("qubits,couple_modes", [([1, 14], True), ([2, 12], True), ([12, 2], True),
+                                                 ([9, 1, 8], True), ([1, 1, 13], True), ([8, 8], True),
+                                                 ([1, 12, 8], False), ([1, 10, 9, 3], False), ([3, 11], True)])
+def test_product_deferral(qubits, couple_modes):
+    """Gates queued after initStateVector that act on one mode alone run on that
+    mode's array before the product is formed (fusion bit 4): equal to the oracle
+    and to the same circuit with deferral off, in both precisions; the modes'
+    transforms ahead of the coupling gates leave the state-wide passes."""
+    from cvdv_b200 import CudaCvdv, _lib
+    rng = np.random.default_rng(sum(qubits) * 13 + len(qubits))
+    sep = _separable(qubits, rng)
+    seq = _deferral_circuit(qubits, rng, couple_modes)
+    o = OracleSim(list(qubits))
+    o.initStateVector(sep)
+    run(o, seq)
+    ref = o.get_state()
+    for prec, tol in (("complex128", PLAIN_TOL), ("complex64", MIXED_TOL)):
+        outs, passes = {}, {}
+        for flags in (31, 15):
+            sim = CudaCvdv(list(qubits), precision=prec, check_errors=True)
+            sim.setFusion(flags)
+            _lib.load().cvdvSetTiming(sim.ctx, 1)
+            sim.initStateVector(sep)
+            run(sim, seq)
+            outs[flags] = sim.getState()
+            st = _lib.kernel_stats(sim.ctx)
+            passes[flags] = st["fft_pass"][1] + st["col"][1]
+            assert st["init"][1] >= 1, (prec, flags, st)
+            assert rel(outs[flags], ref) < tol, (prec, flags, rel(outs[flags], ref))
+        assert rel(outs[31], outs[15]) < tol
+        assert passes[31] < passes[15], (prec, passes)
+
+
+def test_product_deferral_edges():
+    """Readout straight after initStateVector, a second initStateVector replacing
+    the first with its gates, a state read in the middle, and parity of the
+    deferred path with the plain one for a separable-state fidelity."""
+    from cvdv_b200 import CudaCvdv
+    qubits = [1, 12]
+    rng = np.random.default_rng(5)
+    sep1, sep2 = _separable(qubits, rng), _separable(qubits, rng)
+    o = OracleSim(qubits)
+    o.initStateVector(sep1)
+    sim = CudaCvdv(qubits, check_errors=True)
+    sim.initStateVector(sep1)
+    assert rel(sim.getState(), o.get_state()) < 1e-14
+    sim.d(1, 0.5 + 0.2j)
+    sim.initStateVector(sep2)  # replaces the state and drops the queued gate
+    sim.s(1, 0.2)
+    o2 = OracleSim(qubits)
+    o2.initStateVector(sep2)
+    o2.s(1, 0.2)
+    mid = sim.getState()
+    assert rel(mid, o2.get_state()) < PLAIN_TOL
+    sim.ftQ2P(1)
+    sim.cd(1, 0, 0, 0.3)
+    o2.ft_q2p(1)
+    o2.cd(1, 0, 0, 0.3)
+    assert rel(sim.getState(), o2.get_state()) < PLAIN_TOL
+    sim.initStateVector(sep1)
+    sim.r(1, 0.3)
+    o.r(1, 0.3)
+    np.testing.assert_allclose(sim.m(0), o.m(0), atol=1e-13)
+    assert abs(sim.getFidelity(sep1) - o.getFidelity(sep1)) < 1e-12
