@@ -44,7 +44,6 @@ void set_error(Context* ctx, int code, const char* fmt, ...) {
 // ----------------------------------------------------------------- launch accounting
 std::atomic<unsigned long long> g_launches{0};
 static thread_local int t_scopeDepth = 0;
-static thread_local int t_scopeKind = 0;
 
 static cudaEvent_t pool_event(Context* c) {
   if (!c->eventPool.empty()) {
@@ -59,7 +58,6 @@ static cudaEvent_t pool_event(Context* c) {
 
 void launch_begin(Context* c, int kind) {
   if (t_scopeDepth++ > 0) return;  // nested scopes count once
-  t_scopeKind = kind;
   g_launches.fetch_add(1, std::memory_order_relaxed);
   if (c && c->timing) {
     TimingRec r{pool_event(c), pool_event(c), kind};

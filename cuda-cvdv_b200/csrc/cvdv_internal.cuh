@@ -107,8 +107,8 @@ __device__ __forceinline__ double2 dmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-// Evaluate the factor at flat index i (FP64).  Returns false when the list is
-// empty (factor == 1).
+// Evaluate the factor at flat index i (FP64); an empty list gives 1.  XX = false
+// leaves out the bilinear terms (lists the caller knows have none).
 template <int MAXT = kMaxTab, bool XX = true>
 __device__ __forceinline__ double2 eval_factor_t(const FactorList& F, uint64_t i) {
   double2 f = F.hasScalar ? F.scalar : make_double2(1.0, 0.0);
@@ -126,19 +126,20 @@ __device__ __forceinline__ double2 eval_factor_t(const FactorList& F, uint64_t i
 #pragma unroll
   for (int t = 0; t < MAXT; ++t)
     if (t < F.nTab) f = dmul(f, tv[t]);
-  if (!XX) return f;
+  if constexpr (XX) {
 #pragma unroll 1
-  for (int t = 0; t < F.nXX; ++t) {
-    const XXFactor& X = F.xx[t];
-    int j1 = (int)((i >> X.shift1) & (uint64_t)X.mask1);
-    int j2 = (int)((i >> X.shift2) & (uint64_t)X.mask2);
-    double x1 = ((double)j1 - X.c1) * X.dx1;
-    double x2 = ((double)j2 - X.c2) * X.dx2;
-    double ph = X.coeff * x1 * x2;
-    if (X.ctrlShift >= 0 && ((i >> X.ctrlShift) & 1ull)) ph = -ph;
-    double s, c;
-    sincos(ph, &s, &c);
-    f = dmul(f, make_double2(c, s));
+    for (int t = 0; t < F.nXX; ++t) {
+      const XXFactor& X = F.xx[t];
+      int j1 = (int)((i >> X.shift1) & (uint64_t)X.mask1);
+      int j2 = (int)((i >> X.shift2) & (uint64_t)X.mask2);
+      double x1 = ((double)j1 - X.c1) * X.dx1;
+      double x2 = ((double)j2 - X.c2) * X.dx2;
+      double ph = X.coeff * x1 * x2;
+      if (X.ctrlShift >= 0 && ((i >> X.ctrlShift) & 1ull)) ph = -ph;
+      double s, c;
+      sincos(ph, &s, &c);
+      f = dmul(f, make_double2(c, s));
+    }
   }
   return f;
 }

@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_pass(const C* __restrict__ 
                                                          FactorList pre, FactorList post) {
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
-  const int R = 1 << P.logR, B = 1 << P.logB;
+  const int R = 1 << P.logR;
   const int RP = (padt(R) | 1);
   const int logNR = P.logN - P.logR;
   const uint64_t c0 = (uint64_t)blockIdx.x << P.logB;
