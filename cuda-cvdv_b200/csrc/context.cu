@@ -367,18 +367,29 @@ struct Op {
   bool blockedIn = false, blockedOut = false;
 };
 
-static bool xx_touches(const std::vector<Term>& terms, int r) {
-  for (const Term& t : terms)
-    if (t.kind == kTermXX && (t.r == r || t.s == r)) return true;
+// Whether an op reads register r other than through factor tables over r (built
+// permuted while r is blocked): a 2x2 gate on one of r's bits, a control bit
+// inside r for a term on another register, a bilinear term on r.  Those index
+// r's bits directly and need its natural order.
+static bool reads_reg_bits(Context* ctx, const Op& b, int r) {
+  const int lo = ctx->flw[r], hi = lo + ctx->q[r];
+  auto inReg = [&](int bit) { return bit >= lo && bit < hi; };
+  if (b.st && b.st->kind == kStPair && inReg(b.st->bit)) return true;
+  for (const std::vector<Term>* v : {&b.pre, &b.post})
+    for (const Term& t : *v) {
+      if (t.kind == kTermXX && (t.r == r || t.s == r)) return true;
+      if (t.ctrlBit >= 0 && inReg(t.ctrlBit) && t.r != r) return true;
+    }
   return false;
 }
 
 // Pair a row program that ends with a forward 2^14-point transform (two-CTA
 // kernel) with the next row program on the same register that starts with the
 // inverse one, when everything in between only reads that register through
-// factor tables (qubit gates, transforms of other registers, diagonal runs
-// without bilinear terms on it).  The pair keeps the register in the blocked
-// order in between, which saves the two layout swaps.
+// factor tables (qubit gates on other registers, transforms of other registers,
+// diagonal runs without bilinear terms on it or controls inside it).  The pair
+// keeps the register in the blocked order in between, which saves the two
+// layout swaps.
 static void pair_blocked_programs(Context* ctx, std::vector<Op>& ops) {
   for (size_t i = 0; i < ops.size(); ++i) {
     Op& a = ops[i];
@@ -406,7 +417,7 @@ static void pair_blocked_programs(Context* ctx, std::vector<Op>& ops) {
       if (b.rowReg >= 0) break;
       if (b.st && b.st->kind == kStPerm) break;
       if (b.st && b.st->kind == kStFft && b.st->reg == r) break;
-      if (xx_touches(b.pre, r) || xx_touches(b.post, r)) break;
+      if (reads_reg_bits(ctx, b, r)) break;
     }
   }
 }

@@ -689,3 +689,29 @@ def test_product_deferral_edges():
     o.r(1, 0.3)
     np.testing.assert_allclose(sim.m(0), o.m(0), atol=1e-13)
     assert abs(sim.getFidelity(sep1) - o.getFidelity(sep1)) < 1e-12
+
+
+def test_mode_bits_between_paired_transforms():
+    """Gates between a forward and an inverse transform of a 2^14-point mode: the
+    mode may stay in the blocked order only when they read it through factor
+    tables (an Rz on one of its bits); a 2x2 gate on one of its bits or a control
+    inside it for a gate on another register needs the natural order."""
+    qubits = [9, 1, 14]
+    rng = np.random.default_rng(77)
+    n = sum(qubits)
+    psi = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    psi /= np.linalg.norm(psi)
+    seqs = [
+        [("ftQ2P", (2,)), ("h", (2, 0)), ("ftP2Q", (2,))],
+        [("ftQ2P", (2,)), ("h", (1, 0)), ("h", (2, 13)), ("ftP2Q", (2,))],
+        [("ftQ2P", (2,)), ("cd", (0, 2, 3, 0.4j)), ("h", (1, 0)), ("ftP2Q", (2,))],
+        [("ftQ2P", (2,)), ("h", (1, 0)), ("rz", (2, 5, 0.3)), ("ftP2Q", (2,))],
+    ]
+    for seq in seqs:
+        o = oracle(qubits, psi)
+        run(o, seq)
+        ref = o.get_state()
+        for prec, tol in (("complex128", PLAIN_TOL), ("complex64", MIXED_TOL)):
+            sim = make(qubits, psi, prec)
+            run(sim, seq)
+            assert rel(sim.getState(), ref) < tol, (prec, seq)
