@@ -531,7 +531,7 @@ static bool stage_commutes(Context* ctx, const Stage& y, const Stage& x) {
 // qubits run, in queue order, in a one-register complex128 context on this
 // context's stream; qubit registers keep theirs (they join the qubit-gate
 // sequences).  Stages that stay are left in order; the product is formed from
-// the updated arrays.
+// the updated arrays before the flush's first launch (launch_product).
 constexpr int kFactorMinQ = 8, kFactorMaxQ = 14;
 
 static Stage factor_stage(Context* ctx, Stage s, int r) {
@@ -556,7 +556,7 @@ static Stage factor_stage(Context* ctx, Stage s, int r) {
   return s;
 }
 
-static bool form_product(Context* ctx, std::vector<Stage>& stages) {
+static bool run_factors(Context* ctx, std::vector<Stage>& stages, std::vector<const double2*>& arrs) {
   const int R = ctx->numReg;
   std::vector<std::vector<Stage>> per(R);
   std::vector<char> coupled(R, 0);
@@ -578,7 +578,7 @@ static bool form_product(Context* ctx, std::vector<Stage>& stages) {
         if (stage_touches_reg(ctx, s, r)) coupled[r] = 1;
     rest.push_back(std::move(s));
   }
-  std::vector<const double2*> arrs(R);
+  arrs.assign(R, nullptr);
   size_t off = 0;
   for (int r = 0; r < R; ++r) {
     arrs[r] = ctx->factors + off;
@@ -609,9 +609,51 @@ static bool form_product(Context* ctx, std::vector<Stage>& stages) {
       return false;
     }
   }
+  stages.swap(rest);
+  return true;
+}
+
+// Whether the flush's first op on register r is a two-CTA row program that starts
+// (after diagonal runs) with an inverse transform, with everything before it
+// reading r only through factor tables; it is then marked to load r blocked.
+static bool starts_blocked(Context* ctx, std::vector<Op>& ops, int r) {
+  for (Op& b : ops) {
+    if (b.rowReg == r) {
+      int firstDir = 0;
+      for (const HostRowOp& h : b.row)
+        if (h.kind == kRowFft) {
+          firstDir = h.dir;
+          break;
+        }
+      if (firstDir >= 0 || b.blockedIn || !rowc_takes(ctx, r, b.row)) return false;
+      b.blockedIn = true;
+      return true;
+    }
+    if (b.rowReg >= 0) return false;
+    if (b.st && b.st->kind == kStPerm) return false;
+    if (b.st && b.st->kind == kStFft && b.st->reg == r) return false;
+    if (reads_reg_bits(ctx, b, r)) return false;
+  }
+  return false;
+}
+
+// The product of the register arrays.  With blockedReg >= 0 (the last register)
+// that register's array is first put in the blocked order (position h M + k2
+// holds index h + 2 k2, M = N / 2), so the state comes out blocked in it.
+static bool launch_product(Context* ctx, std::vector<const double2*>& arrs, int blockedReg) {
+  if (blockedReg >= 0) {
+    const size_t M = (size_t)1 << (ctx->q[blockedReg] - 1);
+    double2* t = (double2*)arena_alloc(ctx, 2 * M * sizeof(double2));
+    if (!t) return false;
+    for (int h = 0; h < 2; ++h)
+      if (!cuda_ok(ctx, cudaMemcpy2DAsync(t + h * M, sizeof(double2), arrs[blockedReg] + h, 2 * sizeof(double2),
+                                          sizeof(double2), M, cudaMemcpyDeviceToDevice, ctx->stream),
+                   "blocked register array"))
+        return false;
+    arrs[blockedReg] = t;
+  }
   if (!launch_init_product(ctx, arrs.data())) return false;
   ctx->productPending = false;
-  stages.swap(rest);
   return true;
 }
 
@@ -625,14 +667,16 @@ bool flush(Context* ctx) {
   arena_reset(ctx);
   std::vector<Stage> stages;
   stages.swap(ctx->pending);
-  if (ctx->productPending) {
-    if (!form_product(ctx, stages)) {
+  const bool product = ctx->productPending;
+  std::vector<const double2*> arrs;
+  if (product) {
+    if (!run_factors(ctx, stages, arrs)) {
       // the state is lost with the product: later calls report it uninitialised
       ctx->productPending = false;
       ctx->initialized = false;
       return false;
     }
-    if (stages.empty()) return true;
+    if (stages.empty()) return launch_product(ctx, arrs, -1);
   }
   if (ctx->fuseSeq) hoist_pairs_past_transforms(ctx, stages);
   std::vector<Op> ops;
@@ -723,7 +767,7 @@ bool flush(Context* ctx) {
     taken[i] = 1;
     ++i;
   }
-  if (ops.empty()) return run_leftover(ctx, diag);
+  if (ops.empty()) return (!product || launch_product(ctx, arrs, -1)) && run_leftover(ctx, diag);
   if (!diag.empty()) {
     if (ops.back().rowReg >= 0) {
       // (only reachable when the program hit its limits) run the tail alone
@@ -738,6 +782,16 @@ bool flush(Context* ctx) {
     Context* c;
     ~PermReset() { c->permReg = -1; }
   } permReset{ctx};
+  if (product) {
+    // a first program on the last register that reads it blocked gets the product blocked
+    const int last = ctx->numReg - 1;
+    const int blocked = starts_blocked(ctx, ops, last) ? last : -1;
+    if (!launch_product(ctx, arrs, blocked)) return false;
+    if (blocked >= 0) {
+      ctx->permReg = blocked;
+      ctx->permLogC = 1;
+    }
+  }
   for (size_t oi = 0; oi < ops.size(); ++oi) {
     Op& op = ops[oi];
     if (ctx->fuseSeq && op.st && op.st->kind == kStPair) {
