@@ -84,3 +84,64 @@ def test_batch_struct_layouts_match(lib_path):
     from cvdv_b200 import batch
     sizes = batch.struct_sizes()
     assert sizes == (batch.PHASE_DTYPE.itemsize, batch.PROGRAM_DTYPE.itemsize, batch.TASK_DTYPE.itemsize)
+
+
+def test_error_paths_without_device(lib_path):
+    """The reference prints or throws through the C ABI; this library records an
+    error code and message and leaves outputs untouched.  Only argument checks
+    that come before any CUDA call are exercised here: invalid creation
+    arguments, calls on an empty context, null pointers."""
+    lib = ctypes.CDLL(lib_path)
+    vp = ctypes.c_void_p
+    lib.cvdvCreateEx.restype = vp
+    lib.cvdvCreateEx.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+    lib.cvdvGetLastError.restype = ctypes.c_int
+    lib.cvdvGetLastError.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
+    lib.cvdvGetNumRegisters.argtypes = [vp]
+    lib.cvdvGetTotalSize.restype = ctypes.c_size_t
+    lib.cvdvGetTotalSize.argtypes = [vp]
+    lib.cvdvGetNorm.restype = ctypes.c_double
+    lib.cvdvGetNorm.argtypes = [vp]
+    lib.cvdvDisplacement.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double]
+    lib.cvdvInitFromSeparable.argtypes = [vp, ctypes.POINTER(vp), ctypes.c_int]
+    lib.cvdvMeasureMultiple.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_double)]
+    lib.cvdvClearError.argtypes = [vp]
+    lib.cvdvDestroy.argtypes = [vp]
+    lib.cvdvMeasureMultipleNoAlloc.restype = ctypes.c_int
+    lib.cvdvMeasureMultipleNoAlloc.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                                               ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                                               ctypes.POINTER(ctypes.c_double), vp]
+
+    def err(ctx):
+        buf = ctypes.create_string_buffer(256)
+        return lib.cvdvGetLastError(ctx, buf, 256), buf.value.decode()
+
+    def ints(*v):
+        return (ctypes.c_int * len(v))(*v)
+
+    # empty context (context.cu:10-12 of the reference): no registers, no error
+    empty = lib.cvdvCreateEx(0, None, 0)
+    assert empty and err(empty)[0] == 0
+    assert lib.cvdvGetNumRegisters(empty) == 0 and lib.cvdvGetTotalSize(empty) == 1
+    # invalid creation arguments are recorded on the returned handle
+    for n, q, prec in [(65, [1] * 65, 0), (2, [3, 40], 0), (2, [3, 0], 0), (1, [3], 7), (2, [20, 20], 0)]:
+        ctx = lib.cvdvCreateEx(n, ints(*q), prec)
+        code, msg = err(ctx)
+        assert code == 1 and msg.startswith("cvdvCreate"), (n, q, prec, code, msg)
+        lib.cvdvDestroy(ctx)
+    # calls on a context without registers or state: error recorded, output untouched
+    lib.cvdvDisplacement(empty, 0, 0.5, 0.0)
+    assert err(empty)[0] != 0
+    lib.cvdvClearError(empty)
+    assert err(empty) == (0, "")
+    lib.cvdvInitFromSeparable(empty, None, 0)
+    assert err(empty)[0] == 2
+    out = (ctypes.c_double * 2)(7.0, 7.0)
+    lib.cvdvMeasureMultiple(empty, ints(0), 1, out)
+    assert err(empty)[0] != 0 and list(out) == [7.0, 7.0]
+    assert lib.cvdvGetNorm(empty) == 0.0 and err(empty)[0] == 2
+    lib.cvdvDestroy(empty)
+    # the allocation-free marginal rejects null pointers before touching the device
+    assert lib.cvdvMeasureMultipleNoAlloc(None, 0, ints(1), 1, ints(0), 1, out, None) == 1
+    assert list(out) == [7.0, 7.0]
