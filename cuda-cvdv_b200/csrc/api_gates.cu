@@ -320,6 +320,9 @@ CVDVContext* cvdvCreateEx(int numReg, int* numQubits, int precision) {
   size_t cap = 16ull << 20;
   if (cudaMalloc((void**)&c->arena, cap) == cudaSuccess) c->arenaCap = cap;
   else cudaGetLastError();
+  // load the device code of cvdvMeasureMultipleNoAlloc on this device now, so
+  // that its first call takes no device memory (a failure shows up there)
+  no_alloc_prepare(c->device, false);
   return ctx;
 }
 

@@ -598,6 +598,8 @@ static bool run_factors(Context* ctx, std::vector<Stage>& stages, std::vector<co
       f->fuseSeq = ctx->fuseSeq;
       f->colFft = ctx->colFft;
       f->colProg = ctx->colProg;
+      // (transform pairs were cancelled when they were queued on this context, so
+      // cvdvCancelledTransforms already counts them)
       f->pending = std::move(per[r]);
       ok = flush(f) && cuda_ok(f, cudaMemcpyAsync((void*)arrs[r], f->state(), bytes,
                                                    cudaMemcpyDeviceToDevice, f->stream),
@@ -641,20 +643,24 @@ static bool starts_blocked(Context* ctx, std::vector<Op>& ops, int r) {
 // that register's array is first put in the blocked order (position h M + k2
 // holds index h + 2 k2, M = N / 2), so the state comes out blocked in it.
 static bool launch_product(Context* ctx, std::vector<const double2*>& arrs, int blockedReg) {
+  bool ok = true;
   if (blockedReg >= 0) {
     const size_t M = (size_t)1 << (ctx->q[blockedReg] - 1);
     double2* t = (double2*)arena_alloc(ctx, 2 * M * sizeof(double2));
-    if (!t) return false;
-    for (int h = 0; h < 2; ++h)
-      if (!cuda_ok(ctx, cudaMemcpy2DAsync(t + h * M, sizeof(double2), arrs[blockedReg] + h, 2 * sizeof(double2),
+    ok = t != nullptr;
+    for (int h = 0; ok && h < 2; ++h)
+      ok = cuda_ok(ctx, cudaMemcpy2DAsync(t + h * M, sizeof(double2), arrs[blockedReg] + h, 2 * sizeof(double2),
                                           sizeof(double2), M, cudaMemcpyDeviceToDevice, ctx->stream),
-                   "blocked register array"))
-        return false;
-    arrs[blockedReg] = t;
+                   "blocked register array");
+    if (ok) arrs[blockedReg] = t;
   }
-  if (!launch_init_product(ctx, arrs.data())) return false;
+  ok = ok && launch_init_product(ctx, arrs.data());
+  // The register arrays already carry the stages run on them and the rest of the
+  // queue is dropped with the flush, so a product that could not be formed leaves
+  // no valid state: later calls report the state uninitialised.
   ctx->productPending = false;
-  return true;
+  if (!ok) ctx->initialized = false;
+  return ok;
 }
 
 bool flush(Context* ctx) {

@@ -314,8 +314,11 @@ bool ensure_state(Context* ctx);                  // allocate both buffers
 // complex128 context of the one register r of ctx, on ctx's stream (api_gates.cu)
 Context* factor_context(Context* ctx, int r);
 bool flush(Context* ctx);                         // run pending stages
+// scratch address of cvdvMeasureMultipleNoAlloc on device dev (current), with its
+// device code loaded; nullptr on failure (recorded as the last error if report)
+double* no_alloc_prepare(int dev, bool report);
 
-// planner/launch helpers (plan.cu)
+// factor lists of a diagonal run (context.cu)
 bool build_factor_list(Context* ctx, const std::vector<Term>& terms, FactorList* out,
                        std::vector<Term>* leftover);
 

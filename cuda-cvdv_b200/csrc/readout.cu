@@ -760,20 +760,49 @@ static double* g_noAllocPtr[kNoAllocMaxDevices];  // device address per device, 
 // Device address of the scratch array on the current device.  The array's name
 // in host code is only a handle for the runtime; the address the kernels use is
 // looked up once per device, with that device current.
-static double* no_alloc_scratch(int dev) {
+static double* no_alloc_scratch(int dev, bool report) {
   std::lock_guard<std::mutex> lk(g_noAllocMu);
   if (!g_noAllocPtr[dev]) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noAllocScratch);
     if (e != cudaSuccess) {
       cudaGetLastError();
-      set_error(nullptr, kErrCuda, "cvdvMeasureMultipleNoAlloc: scratch lookup on device %d: %s", dev,
-                cudaGetErrorString(e));
+      if (report)
+        set_error(nullptr, kErrCuda, "cvdvMeasureMultipleNoAlloc: scratch lookup on device %d: %s", dev,
+                  cudaGetErrorString(e));
       return nullptr;
     }
     g_noAllocPtr[dev] = (double*)p;
   }
   return g_noAllocPtr[dev];
+}
+
+// Loads, on device dev (current), the part of this library's device code that
+// holds the array and the two kernels the entry point launches, and records the
+// array's address.  Under CUDA's lazy module loading (the default since 12.2)
+// that code is loaded on its first use, which takes device memory (the array and
+// the kernels' code); cvdvCreate / cvdvCreateEx call this for their device so a
+// process that made a context makes its first cvdvMeasureMultipleNoAlloc call
+// without that load.
+static std::atomic<bool> g_noAllocLoaded[kNoAllocMaxDevices];
+
+double* no_alloc_prepare(int dev, bool report) {
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return nullptr;
+  double* p = no_alloc_scratch(dev, report);
+  if (!p || g_noAllocLoaded[dev].load()) return p;
+  cudaFuncAttributes fa{};
+  cudaError_t e = cudaFuncGetAttributes(&fa, k_marg_smem<double2>);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_marg_smem<float2>);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_marg_final);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    if (report)
+      set_error(nullptr, kErrCuda, "cvdvMeasureMultipleNoAlloc: loading its kernels on device %d: %s", dev,
+                cudaGetErrorString(e));
+    return nullptr;
+  }
+  g_noAllocLoaded[dev].store(true);
+  return p;
 }
 
 static bool device_pointer_on(const void* p, int dev) {
@@ -863,13 +892,16 @@ extern "C" int cvdvMeasureMultipleNoAlloc(const void* state, int precision, cons
               "%s: state and probsOut must be aligned device memory of the current device %d", fn, dev);
     return kErrInvalidArg;
   }
-  double* scratch = no_alloc_scratch(dev);
+  double* scratch = no_alloc_prepare(dev, true);
   if (!scratch) return kErrCuda;
   cudaStream_t s = (cudaStream_t)stream;
   const uint64_t n = 1ull << total;
   uint64_t maxBlocks = (n + 255) / 256;
   int blocks = kNoAllocBlocks < maxBlocks ? kNoAllocBlocks : (int)maxBlocks;
   size_t smem = (size_t)bins * sizeof(double);
+  // an error the caller's own earlier CUDA work left pending is theirs: it is
+  // neither reported as this call's nor cleared
+  const cudaError_t before = cudaPeekAtLastError();
   {
     LaunchScope _ls(nullptr, kKReduce);
     if (precision == kC128)
@@ -881,8 +913,9 @@ extern "C" int cvdvMeasureMultipleNoAlloc(const void* state, int precision, cons
     LaunchScope _ls(nullptr, kKReduce);
     k_marg_final<<<(int)((bins + 255) / 256), 256, 0, s>>>(scratch, blocks, bins, probsOut);
   }
-  e = cudaGetLastError();
-  if (e != cudaSuccess) {
+  e = cudaPeekAtLastError();
+  if (e != cudaSuccess && e != before) {
+    cudaGetLastError();
     set_error(nullptr, kErrCuda, "%s: launch: %s", fn, cudaGetErrorString(e));
     return kErrCuda;
   }

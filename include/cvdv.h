@@ -271,8 +271,14 @@ int cvdvBatchRunStage(void* states, int precision, const CvdvBatchTask* tasks, i
  * via cvdvGetLastError(NULL, ...)).  Partial histograms live in a fixed
  * 4.625 MiB device array that every GPU loading the library holds until exit,
  * so marginals are limited to 4096 outcomes (12 qubits); larger ones are
- * rejected.  The first call on a device looks up that array's address and
- * should come before any stream capture.  All calls share the array: calls
+ * rejected.  The array and the two kernels live in the library's device code,
+ * which CUDA loads on a device when it is first used (lazy module loading, the
+ * default since CUDA 12.2); that load takes device memory (the array plus the
+ * kernels' code).  cvdvCreate / cvdvCreateEx do it for their device, so after
+ * any context was made on a device the first call allocates nothing.  In a
+ * process that made none, the first call on a device does that set-up (load,
+ * address lookup): make it before the caller's allocator takes the remaining
+ * memory and before any stream capture.  All calls share the array: calls
  * that overlap on the GPU race. */
 int cvdvMeasureMultipleNoAlloc(const void* state, int precision, const int* numQubits, int numReg,
                                const int* regIdxs, int numRegs, double* probsOut, void* stream);

@@ -5,7 +5,8 @@ Runs the reference project's own ``TorchCvdv`` + ``SeparableState``
 stores their outputs as ``.npz`` fixtures.  The reference checkout is only
 needed when regenerating; the committed fixtures are what the tests read.
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py /path/to/reference
+    CVDV_REFERENCE=/path/to/reference python tests/golden/make_golden.py
 
 Every input is seeded (``numpy.random.default_rng``), so re-running this
 script reproduces the fixtures bit for bit on the same library versions.
@@ -19,7 +20,9 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CVDV_REFERENCE")
+if not REF:
+    sys.exit("usage: make_golden.py /path/to/reference  (or set CVDV_REFERENCE)")
 sys.path.insert(0, REF)
 sys.path.insert(0, HERE)
 

@@ -1,0 +1,69 @@
+"""Accuracy of the complex64 (mixed) form at the configured sizes, against the
+complex128 path on the same inputs (the complex128 path itself matches the
+oracle within 1e-10 relative in tests/test_gpu_parity.py).
+
+Tolerances: state infidelity 1 - |<psi128|psi64>|^2 / (|psi128|^2 |psi64|^2)
+at most 1e-6 (the mixed form's accuracy target); marginals and the Wigner grid
+within 1e-6 absolute.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+INFID_TOL = 1e-6
+READOUT_TOL = 1e-6
+
+
+def _run(circ, prec):
+    from cvdv_b200 import CudaCvdv
+    from cvdv_b200 import workloads as W
+    sim = CudaCvdv(circ["qubits"], precision=prec, check_errors=True)
+    sim.initStateVector(W.separable_arrays(circ, device="cuda"))
+    W.apply(sim, circ["prep"])
+    W.apply(sim, circ["gates"])
+    sim.synchronize()
+    return sim
+
+
+def test_state_transfer_mixed_infidelity_full_size():
+    """[1]*14 + [14] (2^28 amplitudes), the 42-gate circuit from the prepared state."""
+    from cvdv_b200 import workloads as W
+    from cvdv_b200.accuracy import compare_states
+    circ = W.state_transfer()
+    s128 = _run(circ, "complex128")
+    s64 = _run(circ, "complex64")
+    acc = compare_states(s128.stateTensor(), s64.stateTensor())
+    assert acc["infidelity"] <= INFID_TOL, acc
+    assert abs(acc["infidelity_raw"]) <= INFID_TOL, acc
+    regs = list(range(14))
+    for a, b in zip(s128.mEach(regs), s64.mEach(regs)):
+        assert np.abs(a - b).max() < READOUT_TOL
+    # repeating the circuit: the error grows with the number of transforms but
+    # stays inside the target after the bench's default 8 repetitions
+    for _ in range(7):
+        W.apply(s128, circ["gates"])
+        W.apply(s64, circ["gates"])
+    acc8 = compare_states(s128.stateTensor(), s64.stateTensor())
+    assert acc8["infidelity"] <= INFID_TOL, acc8
+
+
+def test_gaussian_network_mixed_accuracy_full_size():
+    """[13, 13] (2^26 amplitudes), all 200 layers, then mode 0's Wigner function on
+    the 256 x 256 grid over [-6, 6]^2 and both position marginals."""
+    from cvdv_b200 import workloads as W
+    from cvdv_b200.accuracy import compare_states, wigner_grid
+    circ = W.gaussian_network()
+    s128 = _run(circ, "complex128")
+    s64 = _run(circ, "complex64")
+    acc = compare_states(s128.stateTensor(), s64.stateTensor())
+    assert acc["infidelity"] <= INFID_TOL, acc
+    for a, b in zip(s128.mEach([0, 1]), s64.mEach([0, 1])):
+        assert np.abs(a - b).max() < READOUT_TOL
+    w128 = wigner_grid(s128.getWigner(0))
+    w64 = wigner_grid(s64.getWigner(0))
+    assert w128.shape == (256, 256)
+    assert np.abs(w64 - w128).max() < READOUT_TOL
+    assert np.abs(w128).max() > 1e-3  # the grid covers the state

@@ -107,6 +107,43 @@ def test_marginals():
     np.testing.assert_allclose(each[1], READ["m_2"], atol=1e-14)
 
 
+def test_measure_multiple_ct_alias():
+    """cvdvMeasureMultipleCT (the reference's cuTENSOR variant, measure.cu:125-256)
+    returns the same column-major joint marginal as cvdvMeasureMultiple."""
+    import ctypes
+    from cvdv_b200 import _lib
+    q = [2, 3, 4]
+    sim = make(q, READ["m_state"])
+    L = _lib.load()
+    for key, regs in (("m_20", (2, 0)), ("m_012", (0, 1, 2)), ("m_1", (1,))):
+        n = int(np.prod([1 << q[r] for r in regs]))
+        a, b = np.zeros(n), np.zeros(n)
+        rc = (ctypes.c_int * len(regs))(*regs)
+        L.cvdvMeasureMultiple(sim.ctx, rc, len(regs), a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        L.cvdvMeasureMultipleCT(sim.ctx, rc, len(regs), b.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        assert sim.last_error()[0] == 0
+        np.testing.assert_array_equal(a, b)
+        shape = tuple(1 << q[r] for r in regs)
+        np.testing.assert_allclose(b.reshape(shape[::-1]).T, READ[key], atol=1e-14, err_msg=key)
+
+
+def test_husimi_overlap_alias():
+    """cvdvGetHusimiQOverlap (bosonic.cu:140-144) is the overlap route of
+    cvdvGetHusimiQ: equal to the oracle's Husimi function."""
+    import ctypes
+    from cvdv_b200 import _lib
+    L = _lib.load()
+    for q, reg, key in (([6, 1], 0, "w_state"), ([2, 5, 2], 1, "w3_state")):
+        sim = make(q, READ[key])
+        o = oracle(q, READ[key])
+        N = 1 << q[reg]
+        out = np.zeros(N * N)
+        L.cvdvGetHusimiQOverlap(sim.ctx, reg, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        assert sim.last_error()[0] == 0
+        np.testing.assert_allclose(out.reshape(N, N), o.husimi(reg), atol=1e-13)
+        np.testing.assert_allclose(out.reshape(N, N), sim.getHusimiQ(reg), atol=1e-14)
+
+
 def test_large_marginal_global_path():
     """> 4096 bins uses the global-atomic path."""
     rng = np.random.default_rng(5)
@@ -588,10 +625,23 @@ def test_full_size_state_transfer_properties():
     for k in range(14):
         p = sim.m(k)
         assert abs(p.sum() - n1) < 1e-10
+    # with the queue optimisations off the pair is not cancelled: both 2^14-point
+    # row programs run on the full state
+    from cvdv_b200 import _lib
+    sim.setFusion(0)
     before = sim.stateTensor().clone()
+    L = _lib.load()
+    L.cvdvSetTiming(sim.ctx, 1)
+    _lib.kernel_stats(sim.ctx)
     sim.ftQ2P(14)
+    mid = sim.stateTensor().clone()
     sim.ftP2Q(14)
     after = sim.stateTensor()
+    st = _lib.kernel_stats(sim.ctx)
+    assert st["fft_pass"][1] == 2, st
+    moved = float(torch.linalg.vector_norm(mid - before) / torch.linalg.vector_norm(before))
+    assert moved > 0.1  # the forward transform did change the state
+    del mid
     err = float(torch.linalg.vector_norm(after - before) / torch.linalg.vector_norm(before))
     assert err < 1e-12
 

@@ -77,6 +77,47 @@ def test_no_alloc_marginal_matches_existing(precision):
     assert abs(got.sum() - 1.0) < 1e-6
 
 
+_FIRST_CALL = r"""
+import ctypes, sys
+import numpy as np, torch
+sys.path.insert(0, sys.argv[1])
+from cvdv_b200 import _lib
+from cvdv_b200.cudaCvdv import CudaCvdv
+q = [2, 6, 4, 8]
+rng = np.random.default_rng(3)
+psi = rng.standard_normal(1 << 20) + 1j * rng.standard_normal(1 << 20)
+sim = CudaCvdv(q)  # any context on the device loads the entry point's device code
+sim.initFromArray(psi / np.linalg.norm(psi))
+L = _lib.load()
+ints = lambda v: (ctypes.c_int * len(v))(*v)
+out = torch.zeros(256, dtype=torch.float64, device="cuda")
+state = L.cvdvGetStateDevicePtr(sim.ctx)
+torch.cuda.synchronize()
+free0 = torch.cuda.mem_get_info()[0]
+code = L.cvdvMeasureMultipleNoAlloc(state, 0, ints(q), 4, ints([3]), 1, ctypes.c_void_p(out.data_ptr()),
+                                    L.cvdvGetStream(sim.ctx))
+torch.cuda.synchronize()
+free1 = torch.cuda.mem_get_info()[0]
+ref = sim.m(3)
+print(code, free0 - free1, float(np.max(np.abs(out.cpu().numpy() - ref))))
+"""
+
+
+def test_no_alloc_first_call_in_fresh_process():
+    """In a new process that made a context on the device, the very first call
+    changes the device's free memory by nothing and matches the marginal."""
+    import os
+    import subprocess
+    import sys
+    pkg = os.path.dirname(os.path.dirname(_lib.__file__))
+    r = subprocess.run([sys.executable, "-c", _FIRST_CALL, pkg], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    code, dfree, err = r.stdout.split()[-3:]
+    assert int(code) == 0
+    assert int(dfree) == 0, f"first call took {dfree} bytes of device memory"
+    assert float(err) < 1e-12
+
+
 def test_no_alloc_rejects_oversized_marginal():
     sim = _state("complex128")
     bins = 1 << (QUBITS[3] + QUBITS[1])  # 16384 > 4096
