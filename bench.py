@@ -563,7 +563,7 @@ def gaussian_c3_accuracy(mq, layers=200, n=256, bound=6.0):
     import torch
     from cvdv_b200 import CudaCvdv
     from cvdv_b200 import workloads as W
-    from cvdv_b200.accuracy import wigner_grid
+    from cvdv_b200.accuracy import wigner_grid, wigner_mean
     circ = W.gaussian_network(layers=layers, mode_qubits=mq)
     sims, wig, marg = {}, {}, {}
     for prec in ("complex128", "complex64"):
@@ -579,13 +579,22 @@ def gaussian_c3_accuracy(mq, layers=200, n=256, bound=6.0):
     del sims
     torch.cuda.empty_cache()
     g128, g64 = wigner_grid(wig["complex128"], n, bound), wigner_grid(wig["complex64"], n, bound)
+    c = wigner_mean(wig["complex128"])
+    h128, h64 = wigner_grid(wig["complex128"], n, bound, c), wigner_grid(wig["complex64"], n, bound, c)
     acc.update({"layers": layers, "against": "the complex128 path on the GPU",
                 "marginal_max_abs_err": max(float(np.abs(a - b).max()) for a, b in zip(marg["complex128"],
                                                                                       marg["complex64"])),
+                "marginal_max": max(float(a.max()) for a in marg["complex128"]),
                 "wigner_native_max_abs_err": float(np.abs(wig["complex64"] - wig["complex128"]).max()),
+                "wigner_native_max_abs": float(np.abs(wig["complex128"]).max()),
                 "wigner_grid": f"{n}x{n} over [-{bound}, {bound}]^2, bilinear FP64 resampling of the native grid",
                 "wigner_grid_max_abs_err": float(np.abs(g64 - g128).max()),
-                "wigner_grid_max_abs": float(np.abs(g128).max())})
+                "wigner_grid_max_abs": float(np.abs(g128).max()),
+                "wigner_grid_note": "200 random displacements walk mode 0 to |alpha| ~ 14, outside the origin square; "
+                                    "the centred grid is the same size around the state's mean (x, p)",
+                "wigner_centred_grid_center": list(c),
+                "wigner_centred_grid_max_abs_err": float(np.abs(h64 - h128).max()),
+                "wigner_centred_grid_max_abs": float(np.abs(h128).max())})
     return acc
 
 

@@ -320,6 +320,12 @@ CVDVContext* cvdvCreateEx(int numReg, int* numQubits, int precision) {
   size_t cap = 16ull << 20;
   if (cudaMalloc((void**)&c->arena, cap) == cudaSuccess) c->arenaCap = cap;
   else cudaGetLastError();
+  if (!cuda_ok(c, cudaHostAlloc((void**)&c->waitErr, 64, cudaHostAllocMapped), "cvdvCreate wait flag")) {
+    c->waitErr = nullptr;
+    c->numReg = 0;
+    return ctx;
+  }
+  *c->waitErr = 0;
   // load the device code of cvdvMeasureMultipleNoAlloc on this device now, so
   // that its first call takes no device memory (a failure shows up there)
   no_alloc_prepare(c->device, false);
@@ -353,6 +359,8 @@ Context* factor_context(Context* ctx, int r) {
   cudaStreamSynchronize(f->stream);  // its twiddle table
   cudaStreamDestroy(f->stream);
   f->stream = ctx->stream;  // stream order keeps its kernels between this context's
+  cudaFreeHost(f->waitErr);
+  f->waitErr = ctx->waitErr;  // its kernels' failed waits show at this context's syncs
   ctx->factorCtx[r] = f;
   return f;
 }
@@ -365,7 +373,8 @@ static void release(Context* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (Context* f : c->factorCtx)
     if (f) {
-      f->stream = nullptr;  // this context's stream, destroyed with it
+      f->stream = nullptr;  // this context's stream and wait flag, released with it
+      f->waitErr = nullptr;
       cvdvDestroy(static_cast<CVDVContext*>(f));
     }
   c->factorCtx.clear();
@@ -387,6 +396,8 @@ static void release(Context* c) {
   if (c->big) cudaFree(c->big);
   c->big = nullptr;
   c->bigCap = 0;
+  if (c->waitErr) cudaFreeHost(c->waitErr);
+  c->waitErr = nullptr;
   if (c->hostScratch) cudaFreeHost(c->hostScratch);
   c->hostScratch = nullptr;
   c->hostScratchCap = 0;
@@ -544,7 +555,7 @@ void cvdvSynchronize(CVDVContext* ctx) {
   if (!ctx) return;
   Context* c = C(ctx);
   if (!flush(c)) return;
-  if (c->stream) cuda_ok(c, cudaStreamSynchronize(c->stream), "cvdvSynchronize");
+  if (c->stream) stream_sync(c, "cvdvSynchronize");
 }
 
 void cvdvFlush(CVDVContext* ctx) {

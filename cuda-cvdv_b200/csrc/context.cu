@@ -103,6 +103,16 @@ bool cuda_ok(Context* ctx, cudaError_t e, const char* what) {
   return false;
 }
 
+bool stream_sync(Context* ctx, const char* what) {
+  if (!cuda_ok(ctx, cudaStreamSynchronize(ctx->stream), what)) return false;
+  if (ctx->waitErr && *(volatile unsigned int*)ctx->waitErr) {
+    *(volatile unsigned int*)ctx->waitErr = 0;
+    set_error(ctx, kErrCuda, "%s: a kernel's wait for its cluster peers timed out; the state is not valid", what);
+    return false;
+  }
+  return true;
+}
+
 // ----------------------------------------------------------------- arena
 // Small per-flush scratch (factor tables, partial sums).  Allocation never
 // invalidates pointers handed out since the last reset: when the arena is full
@@ -640,16 +650,18 @@ static bool starts_blocked(Context* ctx, std::vector<Op>& ops, int r) {
 }
 
 // The product of the register arrays.  With blockedReg >= 0 (the last register)
-// that register's array is first put in the blocked order (position h M + k2
-// holds index h + 2 k2, M = N / 2), so the state comes out blocked in it.
+// that register's array is first put in the blocked order of a cluster of
+// C = 2^rowc_log_cluster() CTAs (position h M + k2 holds index h + C k2, M = N / C),
+// so the state comes out blocked in it.
 static bool launch_product(Context* ctx, std::vector<const double2*>& arrs, int blockedReg) {
   bool ok = true;
   if (blockedReg >= 0) {
-    const size_t M = (size_t)1 << (ctx->q[blockedReg] - 1);
-    double2* t = (double2*)arena_alloc(ctx, 2 * M * sizeof(double2));
+    const int nC = 1 << rowc_log_cluster();
+    const size_t M = ((size_t)1 << ctx->q[blockedReg]) / nC;
+    double2* t = (double2*)arena_alloc(ctx, nC * M * sizeof(double2));
     ok = t != nullptr;
-    for (int h = 0; ok && h < 2; ++h)
-      ok = cuda_ok(ctx, cudaMemcpy2DAsync(t + h * M, sizeof(double2), arrs[blockedReg] + h, 2 * sizeof(double2),
+    for (int h = 0; ok && h < nC; ++h)
+      ok = cuda_ok(ctx, cudaMemcpy2DAsync(t + h * M, sizeof(double2), arrs[blockedReg] + h, nC * sizeof(double2),
                                           sizeof(double2), M, cudaMemcpyDeviceToDevice, ctx->stream),
                    "blocked register array");
     if (ok) arrs[blockedReg] = t;
@@ -795,7 +807,7 @@ bool flush(Context* ctx) {
     if (!launch_product(ctx, arrs, blocked)) return false;
     if (blocked >= 0) {
       ctx->permReg = blocked;
-      ctx->permLogC = 1;
+      ctx->permLogC = rowc_log_cluster();
     }
   }
   for (size_t oi = 0; oi < ops.size(); ++oi) {
@@ -821,7 +833,7 @@ bool flush(Context* ctx) {
       if (!launch_row_program(ctx, op.rowReg, op.row, op.blockedIn, op.blockedOut)) return false;
       if (op.blockedOut) {
         ctx->permReg = op.rowReg;
-        ctx->permLogC = 1;
+        ctx->permLogC = rowc_log_cluster();
       }
       continue;
     }

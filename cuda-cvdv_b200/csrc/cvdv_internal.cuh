@@ -275,9 +275,10 @@ struct Context {
   size_t factorsCap = 0;            // in elements
   std::vector<Context*> factorCtx;  // one-register contexts for them, made on first use
   // Inside one flush, between a forward and an inverse 2^14-point transform of
-  // the last register run by the two-CTA row kernel, that register may be stored
-  // "blocked": position r M + k2 holds logical index r + 2 k2 (the transform's
-  // natural output order).  While permReg >= 0, tables over it are built permuted.
+  // the last register run by a cluster row kernel of C = 2^permLogC CTAs, that
+  // register may be stored "blocked": position r M + k2 (M = N / C) holds logical
+  // index r + C k2 (each CTA's natural output order).  While permReg >= 0, tables
+  // over it are built permuted.
   int permReg = -1;
   int permLogC = 0;
   int nextFtTag = 1;
@@ -285,6 +286,9 @@ struct Context {
 
   int lastErr = kOk;
   std::string lastMsg;
+  // Mapped pinned word a kernel sets when a bounded wait on its cluster peers
+  // gives up; read on the host after every synchronisation (stream_sync).
+  unsigned int* waitErr = nullptr;
 
   uint64_t size() const { return 1ull << totalQbt; }
   void* state() const { return buf[cur]; }
@@ -306,6 +310,8 @@ extern std::atomic<unsigned long long> g_launches;
 
 void set_error(Context* ctx, int code, const char* fmt, ...);
 bool cuda_ok(Context* ctx, cudaError_t e, const char* what);
+// synchronise the context's stream and report a failed kernel-side wait
+bool stream_sync(Context* ctx, const char* what);
 void* arena_alloc(Context* ctx, size_t bytes);   // reset per flush / readout
 void arena_reset(Context* ctx);
 void* big_scratch(Context* ctx, size_t bytes);   // persistent, grown on demand
@@ -361,6 +367,7 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
 // whether launch_row_program runs this program on the two-CTA kernel (which can
 // store and load the blocked layout)
 bool rowc_takes(Context* ctx, int reg, const std::vector<HostRowOp>& ops);
+int rowc_log_cluster();  // log2 CTAs per 2^14-point complex128 row (the blocked layout's permLogC)
 // qubit-gate sequences (kernels_seq.cu): 2x2 gates on up to four bits and the
 // diagonal runs between them in one pass
 constexpr int kSeqMaxBits = 5;  // see seq_max_bits

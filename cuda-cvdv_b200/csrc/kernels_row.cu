@@ -93,6 +93,7 @@ struct RowProgram {
                      // reads the whole row in both CTAs (no swap), or -1
   int logS;          // k_rowr on a strided register: log2 of the amplitudes below it (0: rows)
   const double2* tw;
+  unsigned int* waitErr;  // set when a bounded wait on the cluster peers gives up
   RowOp ops[kMaxRowOps];
   RowDiag diag[kMaxRowDiags];
 };
@@ -919,6 +920,292 @@ static cudaError_t launch_rowc_t(Context* ctx, const RowProgram& P) {
   return cudaLaunchKernelEx(&cfg, kern, (const C*)ctx->state(), (C*)ctx->other(), P);
 }
 
+// ---------------------------------------------------------------- four-CTA register-resident rows
+// A row of N = 4 M points is split over a cluster of four CTAs of M / 16 threads
+// (2^14-point complex128 rows: 4096 points and 256 threads per CTA, 72 KB of
+// shared memory, so CTAs of two clusters share an SM and one row's loads and
+// stores run while the other row's butterflies do).  Every thread keeps 16
+// amplitudes in registers.  With Q = M / 4 and m_i = r Q + t + TPR i for thread t
+// of CTA r (i < 4), two layouts occur:
+//   S ("strips"):     v[4 j1 + i] = x[j1 M + m_i]   (CTA r holds quarter r of
+//                     each quarter-row: coalesced loads and stores)
+//   T ("transposed"): v[w] = X[r + 4 k2] at k2 = t + TPR w   (w < 16)
+// Forward, S -> T: radix-4 butterflies over j1 in registers give
+//   y_k1[m_i] = w_N^{m_i k1} sum_j1 w_4^{j1 k1} x[j1 M + m_i];
+//   thread t hands y_k1[m_i] (k1 != r) to thread t of CTA k1, after which every
+//   thread holds y_r[t + TPR k] for all 16 k, and an M-point DFT of y_r gives
+//   X[r + 4 k2] in the natural Stockham order.
+// Inverse, T -> S: an M-point inverse DFT gives z_r[m] at m = t + TPR w; thread t
+//   hands z_r[m] for CTA q's quarter (w = 4 q + i) to thread t of CTA q, then
+//   x[j1 M + m_i] = sum_k1 w_4^{-j1 k1} w_N^{-m_i k1} z_k1[m_i]   (radix-4 again).
+// So each transform moves 12 of a thread's 16 amplitudes once, and only between
+// threads of the same index: the sender writes them straight into the receiving
+// CTA's shared memory (slot (4 src + i) TPR + t) between two cluster barriers; the
+// 4 it keeps never leave its registers.  Diagonal runs in T read tables stored
+// permuted for four CTAs (position r M + k2 holds index r + 4 k2).
+template <typename C, int LOGM>
+__device__ __forceinline__ void rq_diag(C (&v)[16], const RowDiag& D, uint64_t rowBase, int t, int r,
+                                        bool layoutT) {
+  constexpr int M = 1 << LOGM, TPR = M / 16, Q = M / 4;
+  const double2 rs = D.hasRowF ? eval_factor(D.rowF, rowBase) : make_double2(1.0, 0.0);
+  if (D.tab) {
+    int seg = 0;
+    for (int c = 0; c < D.nCtrl; ++c) seg |= (int)((rowBase >> D.ctrlShift[c]) & 1ull) << c;
+    const double2* tp = D.tab + ((size_t)seg << (LOGM + 2));
+    // T: permuted table at r M + k2; S: natural index j1 M + r Q + t + TPR i
+    const double2* base = layoutT ? tp + r * M + t : tp + r * Q + t;
+#pragma unroll
+    for (int k0 = 0; k0 < 16; k0 += 8) {
+      double2 w[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int kk = k0 + k;
+        w[k] = __ldg(base + (layoutT ? TPR * kk : (kk >> 2) * M + TPR * (kk & 3)));
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        if (D.hasRowF) w[k] = dmul(w[k], rs);
+        v[k0 + k] = cmul(v[k0 + k], fromd<C>(w[k]));
+      }
+    }
+  } else if (D.hasRowF) {
+    const C c = fromd<C>(rs);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) v[k] = cmul(v[k], c);
+  }
+}
+
+// ---- cluster primitives (distributed shared memory pushed by st.async)
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ uint32_t cluster_map(uint32_t a, int rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void cluster_arrive_release() {
+  asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait_acquire() {
+  asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void st_async(uint32_t addr, double2 v, uint32_t bar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f64 [%0], {%1, %2}, [%3];" ::"r"(addr),
+               "d"(v.x), "d"(v.y), "r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ void st_async(uint32_t addr, float2 v, uint32_t bar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f32 [%0], {%1, %2}, [%3];" ::"r"(addr),
+               "f"(v.x), "f"(v.y), "r"(bar)
+               : "memory");
+}
+
+// Bounded wait for the phase `parity` of a local mbarrier.  A wait that gives up
+// (a peer that never delivers: a fault elsewhere) records it in *err and returns,
+// so the kernel still reaches its cluster barriers and ends.
+__device__ __forceinline__ void mbar_wait_bounded(uint32_t bar, uint32_t parity, unsigned int* err) {
+  for (uint32_t it = 0; it < (1u << 22); ++it)
+    if (mbar_try_wait(bar, parity)) return;
+  if (err) atomicOr(err, 1u);
+}
+
+// Thread t hands its 12 amplitudes v[4 q + i] (q != r) to thread t of CTA q, slot
+// (4 r + i) TPR + t of that CTA's buffer, and takes v[4 q + i] from slot
+// (4 q + i) TPR + t of its own, which thread t of CTA q wrote.  The writes are
+// st.async into the peer's shared memory, each completing 16 (complex128) or 8
+// bytes on the peer's mbarrier, which expects 12 TPR amplitudes per exchange; so a
+// CTA waits only for its own data, with no cluster-wide barrier or fence.  The
+// caller has arrived on the cluster barrier once its buffer was free (at start,
+// or after its last local use); the wait here orders the remote writes after
+// every peer's arrival.
+template <typename C, int TPR>
+__device__ __forceinline__ void rq_exchange(C (&v)[16], C* buf, uint32_t bar, uint32_t& parity, int t, int r,
+                                            unsigned int* err) {
+  if (t == 0) mbar_expect_tx(bar, 12u * TPR * (uint32_t)sizeof(C));
+  cluster_wait_acquire();
+  const uint32_t base = smem_addr(buf), rbar = bar;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    if (q == r) continue;
+    const uint32_t dst = cluster_map(base, q), dbar = cluster_map(rbar, q);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) st_async(dst + (uint32_t)(((4 * r + i) * TPR + t) * sizeof(C)), v[4 * q + i], dbar);
+  }
+  mbar_wait_bounded(bar, parity, err);
+  parity ^= 1u;
+#pragma unroll
+  for (int k = 0; k < 16; ++k)
+    if ((k >> 2) != r) v[k] = buf[k * TPR + t];
+  __syncthreads();  // every thread has read its slots before the buffer is reused
+}
+
+template <typename C, int LOGN>
+__global__ void __launch_bounds__(1 << (LOGN - 6), 2)
+    k_rowq(const C* __restrict__ in, C* __restrict__ out, uint64_t nRows, const __grid_constant__ RowProgram P) {
+  constexpr int LOGM = LOGN - 2, M = 1 << LOGM, TPR = M / 16, Q = M / 4;
+  constexpr int RS = M + (M >> 4);
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* sm = reinterpret_cast<C*>(smraw);
+  double2* loM = reinterpret_cast<double2*>(sm + RS);  // w_M^e, e < 64
+  double2* hiM = loM + 64;                              // w_M^(64 h), h < M / 64
+  double2* loN = hiM + (M >> 6);                        // w_N^e, e < 64
+  double2* hiN = loN + 64;                              // w_N^(64 h), h < M / 64
+  __shared__ __align__(8) uint64_t xbar;  // completes when the peers' 12 TPR amplitudes have landed
+  cg::cluster_group cl = cg::this_cluster();
+  const int r = (int)cl.block_rank();
+  const int t = threadIdx.x;
+  const uint32_t bar = smem_addr(&xbar);
+  uint32_t parity = 0;
+  if (t == 0) mbar_init(bar, 1);
+  {
+    const int scM = P.logTwN - LOGM, scN = P.logTwN - LOGN;
+    constexpr int NTAB = 2 * (64 + (M >> 6));
+    for (int i = t; i < NTAB; i += TPR) {
+      const int half = i >= NTAB / 2, j = half ? i - NTAB / 2 : i;
+      const int e = j < 64 ? j : (j - 64) << 6;
+      loM[i] = __ldg(P.tw + ((size_t)e << (half ? scN : scM)));  // loM..hiN are one array
+    }
+  }
+  __syncthreads();  // mbarrier and twiddle tables
+  // A CTA arrives on the cluster barrier when its buffer is free (and, the first
+  // time, its mbarrier set up); each exchange waits for every CTA's arrival before
+  // writing into the peers.  A program that starts with a forward transform
+  // arrives at the start of each row, so the wait comes after the loads and
+  // butterflies; one that starts with an inverse transform uses its buffer for
+  // the local stages first and arrives after them.
+  bool fwdFirst = false;
+  for (int o = 0; o < P.nOps; ++o)
+    if (P.ops[o].kind != kRowDiag) {
+      fwdFirst = P.ops[o].dir > 0;
+      break;
+    }
+  // persistent clusters: cluster c takes rows c, c + nClusters, ...
+  const uint64_t nClusters = gridDim.x >> 2;
+  for (uint64_t row = blockIdx.x >> 2; row < nRows; row += nClusters) {
+    const uint64_t rowBase = row << LOGN;
+    bool arrived = fwdFirst;
+    if (arrived) cluster_arrive_release();
+    C v[16];
+    bool layoutT = P.loadT != 0;
+    if (P.loadT == 2) {  // blocked: X[r + 4 k2] contiguous at r M + k2
+#pragma unroll
+      for (int w = 0; w < 16; ++w) v[w] = in[rowBase + (uint64_t)r * M + t + TPR * w];
+    } else if (P.loadT == 1) {  // transposed from the natural layout (every fourth element)
+#pragma unroll
+      for (int w = 0; w < 16; ++w) v[w] = in[rowBase + r + 4 * (uint64_t)(t + TPR * w)];
+    } else {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) v[k] = in[rowBase + (uint64_t)(k >> 2) * M + r * Q + t + TPR * (k & 3)];
+    }
+
+    for (int o = 0; o < P.nOps; ++o) {
+      const RowOp& op = P.ops[o];
+      if (op.kind == kRowDiag) {
+        rq_diag<C, LOGM>(v, P.diag[op.diag], rowBase, t, r, layoutT);
+      } else if (op.dir > 0) {  // S -> T
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          C a0 = v[i], a1 = v[4 + i], a2 = v[8 + i], a3 = v[12 + i];
+          bf4<C, 1>(a0, a1, a2, a3);
+          const C w1 = tw2<C, 1>(loN, hiN, r * Q + t + TPR * i);
+          const C w2 = cmul(w1, w1);
+          v[i] = a0;
+          v[4 + i] = cmul(a1, w1);
+          v[8 + i] = cmul(a2, w2);
+          v[12 + i] = cmul(a3, cmul(w2, w1));
+        }
+        if (!arrived) cluster_arrive_release();  // this CTA is done with its buffer
+        rq_exchange<C, TPR>(v, sm, bar, parity, t, r, P.waitErr);
+        arrived = false;
+        rr_stages<C, 1, LOGM, 0, 4>(v, sm, t, loM, hiM);
+        layoutT = true;
+      } else {  // T -> S
+        rr_stages<C, -1, LOGM, 0, 4>(v, sm, t, loM, hiM);
+        if (!arrived) cluster_arrive_release();
+        rq_exchange<C, TPR>(v, sm, bar, parity, t, r, P.waitErr);
+        arrived = false;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const C w1 = tw2<C, -1>(loN, hiN, r * Q + t + TPR * i);
+          const C w2 = cmul(w1, w1);
+          C a0 = v[i], a1 = cmul(v[4 + i], w1), a2 = cmul(v[8 + i], w2), a3 = cmul(v[12 + i], cmul(w2, w1));
+          bf4<C, -1>(a0, a1, a2, a3);
+          v[i] = a0;
+          v[4 + i] = a1;
+          v[8 + i] = a2;
+          v[12 + i] = a3;
+        }
+        layoutT = false;
+      }
+    }
+
+    if (arrived) cluster_wait_acquire();  // pair an arrival no exchange waited for
+    if (!layoutT) {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) out[rowBase + (uint64_t)(k >> 2) * M + r * Q + t + TPR * (k & 3)] = v[k];
+    } else if (P.storeBlocked) {
+#pragma unroll
+      for (int w = 0; w < 16; ++w) out[rowBase + (uint64_t)r * M + t + TPR * w] = v[w];
+    } else {
+#pragma unroll
+      for (int w = 0; w < 16; ++w) out[rowBase + r + 4 * (uint64_t)(t + TPR * w)] = v[w];
+    }
+    // The next row's first arrival says this CTA's buffer is free again: the last
+    // reads of it (the last exchange or stage) ended in a CTA barrier.
+  }
+}
+template <typename C, int LOGN>
+static cudaError_t launch_rowq_t(Context* ctx, const RowProgram& P) {
+  constexpr int M = 1 << (LOGN - 2);
+  const size_t smem = (size_t)(M + (M >> 4)) * sizeof(C) + 2 * (64 + (M >> 6)) * sizeof(double2);
+  auto kern = k_rowq<C, LOGN>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const uint64_t nRows = ctx->size() >> LOGN;
+  cudaLaunchConfig_t cfg{};
+  cfg.blockDim = dim3(M / 16);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 4;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  // as many clusters as are resident at once (asked once per device), each
+  // walking its share of the rows
+  static int clusters[64] = {};
+  const int dev = ctx->device >= 0 && ctx->device < 64 ? ctx->device : 0;
+  if (!clusters[dev]) {
+    cfg.gridDim = dim3((unsigned)(4 * 1024));
+    int n = 0;
+    e = cudaOccupancyMaxActiveClusters(&n, kern, &cfg);
+    if (e != cudaSuccess) return e;
+    clusters[dev] = n > 0 ? n : 1;
+  }
+  const uint64_t nc = nRows < (uint64_t)clusters[dev] ? nRows : (uint64_t)clusters[dev];
+  cfg.gridDim = dim3((unsigned)(4 * nc));
+  return cudaLaunchKernelEx(&cfg, kern, (const C*)ctx->state(), (C*)ctx->other(), nRows, P);
+}
+
 // ---------------------------------------------------------------- host side
 int row_log_tile(int precision) { return precision == kC128 ? 12 : 13; }
 
@@ -1050,6 +1337,17 @@ static bool rowc_shape(Context* ctx, int reg, const std::vector<HostRowOp>& ops)
   return true;
 }
 
+// log2 of the cluster that runs 2^14-point complex128 row programs: 2 (k_rowq,
+// four 256-thread CTAs) or, with CVDV_ROW_CLUSTER=2 in the environment, 1 (k_rowc,
+// two 512-thread CTAs); the blocked layout between paired programs follows it.
+int rowc_log_cluster() {
+  static const int lc = [] {
+    const char* e = getenv("CVDV_ROW_CLUSTER");
+    return (e && atoi(e) == 2) ? 1 : 2;
+  }();
+  return lc;
+}
+
 bool rowc_takes(Context* ctx, int reg, const std::vector<HostRowOp>& ops) {
   if (!rowc_shape(ctx, reg, ops)) return false;
   for (const HostRowOp& h : ops) {
@@ -1074,8 +1372,8 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
   int logT = q <= row_log_tile(ctx->precision) ? 8 : 9;
   int lt = row_log_tile(ctx->precision) + (logT - 8);
   int logC = q > lt ? q - lt : 0;
-  const bool useC = !col && rowc_takes(ctx, reg, ops);  // the two-CTA register-resident kernel
-  if (useC) logC = 1;
+  const bool useC = !col && rowc_takes(ctx, reg, ops);  // the cluster register-resident kernels
+  if (useC) logC = rowc_log_cluster();
   if (col) logC = 0;
   // k_rowr runs the program when every per-element factor is a linear phase
   bool toRowr = logC == 0 && q <= rowr_max_log(ctx->precision);
@@ -1097,6 +1395,7 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
   P.logTwN = 0;
   while ((1 << P.logTwN) < ctx->twN) ++P.logTwN;
   P.tw = ctx->twiddle;
+  P.waitErr = ctx->waitErr;
   // Layout at every op, as the kernel will see it: a program whose first
   // transform is inverse starts transposed; a forward transform leaves the
   // cluster transposed, an inverse natural; the tail runs in the final layout.
@@ -1196,7 +1495,7 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
     if (blockedIn) P.loadT = 2;
     P.storeBlocked = blockedOut ? 1 : 0;
     P.dualHead = -1;
-    if (P.loadT == 0) {
+    if (P.loadT == 0 && logC == 1) {
       int f = 0;
       while (f < P.nOps && P.ops[f].kind == kRowDiag) ++f;
       if (f < P.nOps && f <= 2 && P.ops[f].dir > 0) P.dualHead = f;
@@ -1204,7 +1503,7 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
     cudaError_t er;
     {
       LaunchScope _ls(ctx, kKFft);
-      er = launch_rowc_t<double2, 14, 4>(ctx, P);
+      er = logC == 2 ? launch_rowq_t<double2, 14>(ctx, P) : launch_rowc_t<double2, 14, 4>(ctx, P);
     }
     if (!cuda_ok(ctx, er, "row program launch")) return false;
     ctx->cur ^= 1;

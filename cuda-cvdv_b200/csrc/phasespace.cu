@@ -364,7 +364,7 @@ static void husimi_wigner_route(Context* c, int r, double* husimiOut) {
   if (!cuda_ok(c, cudaMemcpyAsync(husimiOut, dOut, NN * sizeof(double), cudaMemcpyDeviceToHost,
                                   c->stream), "husimi copy"))
     return;
-  cuda_ok(c, cudaStreamSynchronize(c->stream), "husimi sync");
+  stream_sync(c, "husimi sync");
 }
 
 static void husimi_overlap_route(Context* c, int r, double* husimiOut) {
@@ -422,7 +422,7 @@ static void husimi_overlap_route(Context* c, int r, double* husimiOut) {
   if (!cuda_ok(c, cudaMemcpyAsync(husimiOut, dOut, NN * sizeof(double), cudaMemcpyDeviceToHost,
                                   c->stream), "husimi copy"))
     return;
-  cuda_ok(c, cudaStreamSynchronize(c->stream), "husimi sync");
+  stream_sync(c, "husimi sync");
 }
 
 // The reference chooses the Wigner route when the overlap route's buffers would
@@ -452,7 +452,7 @@ void cvdvGetWigner(CVDVContext* ctx, int regIdx, double* wignerOut) {
   if (!cuda_ok(c, cudaMemcpyAsync(wignerOut, dOut, NN * sizeof(double), cudaMemcpyDeviceToHost,
                                   c->stream), "wigner copy"))
     return;
-  cuda_ok(c, cudaStreamSynchronize(c->stream), "wigner sync");
+  stream_sync(c, "wigner sync");
 }
 
 void cvdvGetHusimiQ(CVDVContext* ctx, int regIdx, double* husimiOut) {

@@ -136,7 +136,7 @@ static bool reduce(Context* ctx, Op op, uint64_t n, double2* result) {
                                     ctx->stream),
                "reduce copy"))
     return false;
-  if (!cuda_ok(ctx, cudaStreamSynchronize(ctx->stream), "reduce sync")) return false;
+  if (!stream_sync(ctx, "reduce sync")) return false;
   *result = make_double2(hs[0], hs[1]);
   return true;
 }
@@ -492,7 +492,7 @@ void cvdvGetState(CVDVContext* ctx, double* realOut, double* imagOut) {
                                     c->stream), "getState copy im"))
       return;
   }
-  cuda_ok(c, cudaStreamSynchronize(c->stream), "getState sync");
+  stream_sync(c, "getState sync");
 }
 
 double cvdvGetNorm(CVDVContext* ctx) {
@@ -536,7 +536,7 @@ static bool measure(Context* c, const int* regIdxs, int numRegs, double* probsOu
   if (!cuda_ok(c, cudaMemcpyAsync(probsOut, dOut, (size_t)outSize * sizeof(double),
                                   cudaMemcpyDeviceToHost, c->stream), "marginal copy"))
     return false;
-  return cuda_ok(c, cudaStreamSynchronize(c->stream), "marginal sync");
+  return stream_sync(c, "marginal sync");
 }
 
 void cvdvMeasureMultiple(CVDVContext* ctx, const int* regIdxs, int numRegs, double* probsOut) {
@@ -596,7 +596,7 @@ void cvdvMeasureEach(CVDVContext* ctx, const int* regIdxs, int numRegs, double* 
       return;
     src += b;
   }
-  cuda_ok(c, cudaStreamSynchronize(c->stream), "marginal sync");
+  stream_sync(c, "marginal sync");
 }
 
 void cvdvGetFidelity(CVDVContext* ctx, void** devicePtrs, int numReg, double* fidOut) {
@@ -695,7 +695,7 @@ void cvdvFidelityStatevectors(CVDVContext* ctx1, CVDVContext* ctx2, double* fidO
     return;
   }
   if (!ready(a, "cvdvFidelityStatevectors") || !ready(b, "cvdvFidelityStatevectors")) return;
-  if (a != b && !cuda_ok(b, cudaStreamSynchronize(b->stream), "fidelity sync")) return;
+  if (a != b && !stream_sync(b, "fidelity sync")) return;
   arena_reset(a);
   double2 ip;
   bool ok;

@@ -8,8 +8,9 @@ complex64) in chunks, accumulating in complex128 on the GPU:
   rel_l2        ||psi - ref|| / ||ref||
 
 ``wigner_grid`` resamples a native N x N Wigner array (row p, column x, the
-layout of ``CudaCvdv.getWigner``) onto an n x n grid over [-bound, bound]^2 by
-bilinear interpolation in FP64 on the native lattice
+layout of ``CudaCvdv.getWigner``) onto an n x n grid over [-bound, bound]^2
+(optionally shifted to a centre, e.g. ``wigner_mean``) by bilinear
+interpolation in FP64 on the native lattice
   x_j = (j - (N-1)/2) dx,  p_k = (k - N/2) pi / (N dx),  dx = sqrt(2 pi / N)
 (src/cudaCvdv.py:186-197 gives the native lattice).  The same deterministic
 map applied to two native arrays gives grids whose difference is bounded by the
@@ -62,16 +63,27 @@ def _weights(axis: np.ndarray, pts: np.ndarray):
     return i0, f
 
 
-def wigner_grid(W: np.ndarray, n: int = 256, bound: float = 6.0) -> np.ndarray:
-    """Bilinear FP64 resampling of a native Wigner array onto n x n points
-    linspace(-bound, bound, n) in p (rows) and x (columns)."""
+def wigner_mean(W: np.ndarray):
+    """(<x>, <p>) of a native Wigner array: sum x W / sum W and sum p W / sum W."""
     N = W.shape[0]
     x, p = native_axes(N)
-    pts = np.linspace(-bound, bound, n)
-    if pts[0] < max(x[0], p[0]) or pts[-1] > min(x[-1], p[-1]):
-        raise ValueError("bound outside the native grid")
-    ix, fx = _weights(x, pts)
-    ip, fp = _weights(p, pts)
+    W = np.asarray(W, dtype=np.float64)
+    tot = W.sum()
+    return float((W.sum(axis=0) * x).sum() / tot), float((W.sum(axis=1) * p).sum() / tot)
+
+
+def wigner_grid(W: np.ndarray, n: int = 256, bound: float = 6.0, center=(0.0, 0.0)) -> np.ndarray:
+    """Bilinear FP64 resampling of a native Wigner array onto n x n points
+    center + linspace(-bound, bound, n) in p (rows) and x (columns); center is
+    (x0, p0)."""
+    N = W.shape[0]
+    x, p = native_axes(N)
+    px = center[0] + np.linspace(-bound, bound, n)
+    pp = center[1] + np.linspace(-bound, bound, n)
+    if px[0] < x[0] or px[-1] > x[-1] or pp[0] < p[0] or pp[-1] > p[-1]:
+        raise ValueError("grid outside the native grid")
+    ix, fx = _weights(x, px)
+    ip, fp = _weights(p, pp)
     W = np.asarray(W, dtype=np.float64)
     top = W[ip][:, ix] * (1 - fx) + W[ip][:, ix + 1] * fx
     bot = W[ip + 1][:, ix] * (1 - fx) + W[ip + 1][:, ix + 1] * fx
