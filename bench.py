@@ -514,8 +514,12 @@ def gaussian_c3(args):
     mq = 13 if args.workload == "full" else 12
     circ = W.gaussian_network(layers=layers, mode_qubits=mq)
     out = {"unit": "layers/s", "layers_per_step": layers, "gates_per_layer": len(circ["gates"]) // layers}
-    for prec in ("complex128", "complex64"):
-        sim = CudaCvdv(circ["qubits"], precision=prec, check_errors=True)
+    # complex64_tensor_core: the same complex64 run with mode 0's transforms as
+    # chained four-step passes of DFT-matrix products on the tensor cores (fusion
+    # bit 5, opt-in) instead of the one-pass column programs
+    for prec, label, flags in (("complex128", "complex128", 31), ("complex64", "complex64", 31),
+                               ("complex64", "complex64_tensor_core", 63)):
+        sim = CudaCvdv(circ["qubits"], precision=prec, check_errors=True, fusion=flags)
         sim.initStateVector(W.separable_arrays(circ, device="cuda"))
         W.apply(sim, circ["prep"])
         W.apply(sim, circ["gates"])  # warm-up
@@ -540,14 +544,15 @@ def gaussian_c3(args):
         kern = {k: {"ms_per_layer": v[0] / layers, "launches_per_layer": v[1] / layers}
                 for k, v in st.items() if v[1]}
         state_bytes = (16 if prec == "complex128" else 8) << sum(circ["qubits"])
-        if "col" in kern:  # one column pass reads and writes the state once
-            avg = kern["col"]["ms_per_layer"] / kern["col"]["launches_per_layer"]
-            kern["col"]["achieved_gbs"] = 2 * state_bytes / (avg * 1e-3) / 1e9
+        for k in ("col", "col_tc"):  # one column pass reads and writes the state once
+            if k in kern:
+                avg = kern[k]["ms_per_layer"] / kern[k]["launches_per_layer"]
+                kern[k]["achieved_gbs"] = 2 * state_bytes / (avg * 1e-3) / 1e9
         t0 = time.perf_counter()
         w = sim.getWigner(0)
         wig_s = time.perf_counter() - t0
-        out[prec] = {"value": 1e3 / ms, "ms_per_layer": ms, "wigner_s": wig_s, "wigner_shape": list(w.shape),
-                     "kernels": kern}
+        out[label] = {"value": 1e3 / ms, "ms_per_layer": ms, "wigner_s": wig_s, "wigner_shape": list(w.shape),
+                      "kernels": kern}
         del sim
         torch.cuda.empty_cache()
     out["value"] = out["complex128"]["value"]
@@ -566,16 +571,18 @@ def gaussian_c3_accuracy(mq, layers=200, n=256, bound=6.0):
     from cvdv_b200.accuracy import wigner_grid, wigner_mean
     circ = W.gaussian_network(layers=layers, mode_qubits=mq)
     sims, wig, marg = {}, {}, {}
-    for prec in ("complex128", "complex64"):
-        sim = CudaCvdv(circ["qubits"], precision=prec, check_errors=True)
+    for prec, label, flags in (("complex128", "complex128", 31), ("complex64", "complex64", 31),
+                               ("complex64", "tc", 63)):
+        sim = CudaCvdv(circ["qubits"], precision=prec, check_errors=True, fusion=flags)
         sim.initStateVector(W.separable_arrays(circ, device="cuda"))
         W.apply(sim, circ["prep"])
         W.apply(sim, circ["gates"])
         sim.synchronize()
-        sims[prec] = sim
-        marg[prec] = sim.mEach([0, 1])
-        wig[prec] = sim.getWigner(0)
+        sims[label] = sim
+        marg[label] = sim.mEach([0, 1])
+        wig[label] = sim.getWigner(0) if label != "tc" else None
     acc = compare_states(sims["complex128"].stateTensor(), sims["complex64"].stateTensor())
+    acc["tensor_core_columns"] = compare_states(sims["complex128"].stateTensor(), sims["tc"].stateTensor())
     del sims
     torch.cuda.empty_cache()
     g128, g64 = wigner_grid(wig["complex128"], n, bound), wigner_grid(wig["complex64"], n, bound)

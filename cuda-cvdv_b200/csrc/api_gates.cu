@@ -398,6 +398,10 @@ static void release(Context* c) {
   c->bigCap = 0;
   if (c->waitErr) cudaFreeHost(c->waitErr);
   c->waitErr = nullptr;
+  for (void*& p : c->tcImage) {
+    if (p) cudaFree(p);
+    p = nullptr;
+  }
   if (c->hostScratch) cudaFreeHost(c->hostScratch);
   c->hostScratch = nullptr;
   c->hostScratchCap = 0;
@@ -583,6 +587,7 @@ void cvdvSetFusion(CVDVContext* ctx, int flags) {
   C(ctx)->colFft = (flags & 4) != 0;
   C(ctx)->colProg = (flags & 8) != 0;
   C(ctx)->deferProduct = (flags & 16) != 0;
+  C(ctx)->tcCol = (flags & 32) != 0;
 }
 
 long long cvdvCancelledTransforms(CVDVContext* ctx) { return ctx ? C(ctx)->ftCancelled * 2 : 0; }

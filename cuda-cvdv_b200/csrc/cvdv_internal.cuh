@@ -207,7 +207,8 @@ enum KernelKind : int {
   kKPhaseSpace = 7,
   kKSeq = 8,
   kKCol = 9,
-  kKindCount = 10,
+  kKColTc = 10,  // column passes on the tensor cores
+  kKindCount = 11,
 };
 
 struct TimingRec {
@@ -265,6 +266,8 @@ struct Context {
   bool fuseSeq = true;  // run chains of qubit gates as one qubit-gate sequence pass
   bool colFft = true;   // transforms of strided registers by the register-resident column kernel
   bool colProg = true;  // programs on strided registers by the register-resident row kernel in column form
+  bool tcCol = false;   // complex64 column passes of 2^12..2^14-point registers on the tensor cores (opt-in)
+  void* tcImage[2] = {nullptr, nullptr};  // their DFT matrices (64-point blocks, 128-point), made on first use
   // Product deferral (on by default, cvdvSetFusion bit 4): cvdvInitFromSeparable
   // keeps the register arrays and the next flush forms the product, after the
   // queued stages that act on one register alone, ahead of every stage that
@@ -342,6 +345,7 @@ bool launch_perm(Context* ctx, const Stage& st, const FactorList& pre, const Fac
 bool launch_fft(Context* ctx, int reg, int dir, const FactorList& pre, const FactorList& post);
 bool col_fft_ok(Context* ctx, int reg);
 bool col_program_ok(Context* ctx, int reg);
+bool tc_col_ok(Context* ctx, int reg);  // kernels_tc.cu
 bool launch_col_fft(Context* ctx, int reg, int dir, const FactorList& pre, const FactorList& post);
 bool launch_fft_generic(Context* ctx, const void* in, void* out, void* tmp, uint64_t O,
                         int q, uint64_t S, int dir, int prec);
@@ -364,7 +368,7 @@ bool launch_col_chain(Context* ctx, int reg, const std::vector<HostRowOp>& ops);
 // inverse transform; blockedOut: leave it blocked after the final forward transform
 bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops, bool blockedIn = false,
                         bool blockedOut = false);
-// whether launch_row_program runs this program on the two-CTA kernel (which can
+// whether launch_row_program runs this program on the four-CTA kernel (which can
 // store and load the blocked layout)
 bool rowc_takes(Context* ctx, int reg, const std::vector<HostRowOp>& ops);
 int rowc_log_cluster();  // log2 CTAs per 2^14-point complex128 row (the blocked layout's permLogC)

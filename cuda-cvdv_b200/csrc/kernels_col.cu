@@ -23,43 +23,11 @@
 // diagonal run between, and pass 1 of transform t + 1 run on one column load --
 // T transforms take T + 1 passes instead of 2T.
 
+#include "col_pass.cuh"
 #include "cvdv_internal.cuh"
 #include "row_fft.cuh"
 
 namespace cvdv {
-
-constexpr int kColThreads = 256;
-constexpr int kMaxColOps = 24;
-constexpr int kMaxColDiags = 10;
-
-enum ColOpKind : int { kColDft = 0, kColDiag = 1 };
-
-struct ColOp {
-  int kind;
-  int dir;   // DFT: +1 forward, -1 inverse
-  int diag;  // diagonal run: index into ColPass::diag
-};
-
-struct ColPass {
-  uint64_t nCols;
-  int logS;           // inner size S = 2^logS
-  int logA;           // log2 of the middle index range of a column's base
-  uint64_t midIn, outerIn, axisIn;     // strides (amplitudes) of the input
-  uint64_t midOut, outerOut, axisOut;  // strides of the output
-  int logN;           // four-step twiddle: multiply point m of column (mid) by w_N^{mid m}
-  int logTwN;
-  const double2* tw;  // w_{2^logTwN}^e table of the context
-  int nOps, nDiag;
-  ColOp ops[kMaxColOps];
-  // diagonal runs, evaluated at input addresses before the first DFT, output ones
-  // after: diag[d] per point, and the run's bilinear terms c x_reg x_other (control
-  // bit off the register) lin[d][0..nLin[d]) as a linear phase along the column
-  FactorList diag[kMaxColDiags];
-  int nLin[kMaxColDiags];
-  XXFactor lin[kMaxColDiags][kMaxXX];  // side 1: the other register
-  int logQ;            // register length 2^logQ
-  double regC, regDx;  // centre and spacing of the register's grid
-};
 
 // CE: log2 of the points a thread holds (16 or 8); the shared line of a column is
 // padded once per radix (16 or 8 points) and has an odd length, so the W columns
@@ -76,10 +44,6 @@ struct ColShape {
 // complex128 pass of a 2^26-amplitude state, 0.54 against 0.65 in complex64
 template <typename C> struct ColCE { static constexpr int v = 3; };
 
-// Pass shapes: the first half of a transform (diagonal runs on the loads, DFT,
-// four-step twiddle), a shared middle pass (DFT, runs, DFT, twiddle), the second
-// half (DFT, runs on the stores), or a whole run on a short register (the op list).
-enum ColKind : int { kColFirst = 0, kColMiddle = 1, kColLast = 2, kColWhole = 3 };
 
 // The linear phase of diagonal run d on the points t + TPC k (k < E) of a column
 // whose point m sits at b + m ax: a (j - regC) regDx at register index j = j0 + u m,
@@ -254,6 +218,8 @@ static cudaError_t col_dispatch(Context* ctx, int logL, const ColPass& P, int ki
   }
 }
 
+cudaError_t launch_col_tc(Context* ctx, const ColPass& P, int logL, int kind, int d1, int d2);  // kernels_tc.cu
+
 // Whether the column kernel takes transforms of register `reg`: 2^4..2^16 points
 // and at least 8 amplitudes below it (runs of 8 contiguous columns for the loads
 // and stores).  A pass of 2^l points has 2^(n-l) columns and 2^(11-l) columns per
@@ -336,9 +302,14 @@ static bool run_col_chain(Context* ctx, int reg, const std::vector<int>& dirs,
       if ((!factor_empty(F.F) || F.nLin) && !add_op(P, kColDiag, 0, &F)) return false;
     return true;
   };
+  // complex64 passes of 64 or 128 points run as DFT-matrix products on the tensor cores
+  const bool tc = tc_col_ok(ctx, reg);
   auto go = [&](const ColPass& P, int logL, int kind, int d1, int d2) -> bool {
     cudaError_t e;
-    {
+    if (tc && kind != kColWhole && (logL == 6 || logL == 7) && P.logA >= 7 - logL) {
+      LaunchScope _ls(ctx, kKColTc);
+      e = launch_col_tc(ctx, P, logL, kind, d1, d2);
+    } else {
       LaunchScope _ls(ctx, kKCol);
       e = ctx->precision == kC128 ? col_dispatch<double2>(ctx, logL, P, kind, d1, d2)
                                   : col_dispatch<float2>(ctx, logL, P, kind, d1, d2);

@@ -88,9 +88,7 @@ struct RowProgram {
   int nDiag;
   int logTwN;
   int loadT;    // cluster rows: start transposed (1: from the natural layout, 2: from the blocked one)
-  int storeBlocked;  // two-CTA rows ending transposed: write the blocked layout
-  int dualHead;      // two-CTA rows: index of a leading forward transform whose radix-2 step
-                     // reads the whole row in both CTAs (no swap), or -1
+  int storeBlocked;  // four-CTA rows ending transposed: write the blocked layout
   int logS;          // k_rowr on a strided register: log2 of the amplitudes below it (0: rows)
   const double2* tw;
   unsigned int* waitErr;  // set when a bounded wait on the cluster peers gives up
@@ -652,272 +650,10 @@ bool col_program_ok(Context* ctx, int reg) {
   if (!ctx->colProg || ctx->precision != kC64 || ctx->flw[reg] == 0 || q <= 8 ||
       q > rowr_max_log(ctx->precision))
     return false;
+  if (ctx->colFft && col_fft_ok(ctx, reg) && tc_col_ok(ctx, reg)) return false;  // chained tensor-core passes
   const int logE = (ctx->precision == kC64 && q >= 13) ? 5 : 4;
   const int logR = q - logE < 8 ? 8 - (q - logE) : 0;
   return ctx->totalQbt - q >= logR;
-}
-
-// ---------------------------------------------------------------- two-CTA register-resident rows
-// A row of N = 2 M points (2^14) is split over a cluster of two CTAs of M/E
-// threads; every thread keeps E amplitudes in registers (E = 16 complex128,
-// 32 complex64).  With H = E/2 and m_i = t + TPR (H r + i), i < H, for thread t
-// of CTA r, two layouts occur:
-//   S ("split natural"): v[i] = x[m_i], v[H + i] = x[M + m_i];
-//   T ("transposed"):    v[w] = X[r + 2 k2] at k2 = t + TPR w (all E w).
-// Forward DFT, S -> T:  y_k1[m] = w_N^{m k1} (x[m] + (-1)^k1 x[M + m]); each CTA
-//   forms both y_0 and y_1 on its own m_i, keeps y_r and hands y_(1-r) to the
-//   sibling through distributed shared memory (8 values per thread); then an
-//   M-point DFT of y_r gives X[r + 2 k2].
-// Inverse DFT, T -> S:  an M-point inverse DFT gives z_r[m] (all 16 w); each CTA
-//   hands the sibling the half of z_r it needs and forms
-//   x[m_i] = z_0 + w_N^{-m} z_1, x[M + m_i] = z_0 - w_N^{-m} z_1.
-// Loads and stores in S are plain coalesced accesses; a program that starts
-// (ends) in T loads (stores) adjacent pairs X[2 k2], X[2 k2 + 1] for the CTA's
-// half of k2 and swaps one of each pair with the sibling.  Diagonal runs in T
-// read tables stored permuted (position r M + k2 holds index r + 2 k2).
-
-// Hand the sibling 8 registers and take 8 of its: this CTA writes its registers
-// SEND_HI (w = 8 SEND_HI + i) at their canonical positions, the sibling does the
-// same, and each reads the other's.  Both CTAs call it with mirrored halves.
-template <typename C, int TPR, int H>
-__device__ __forceinline__ void rc_swap(C* sm, const C* peer, int t, const C (&send)[H], C (&recv)[H],
-                                       int sendHalf, int recvHalf) {
-  cg::cluster_group cl = cg::this_cluster();
-#pragma unroll
-  for (int i = 0; i < H; ++i) sm[rpad<C>(t + TPR * (H * sendHalf + i))] = send[i];
-  cl.sync();
-#pragma unroll
-  for (int i = 0; i < H; ++i) recv[i] = peer[rpad<C>(t + TPR * (H * recvHalf + i))];
-  cl.sync();  // the sibling has read this CTA's buffer before it is reused
-}
-
-template <typename C, int LOGM, int LOGE>
-__device__ __forceinline__ void rc_diag(C (&v)[1 << LOGE], const RowDiag& D, uint64_t rowBase, int t, int r,
-                                        bool layoutT) {
-  constexpr int E = 1 << LOGE, H = E / 2, TPR = 1 << (LOGM - LOGE), M = 1 << LOGM;
-  const double2 rs = D.hasRowF ? eval_factor(D.rowF, rowBase) : make_double2(1.0, 0.0);
-  if (D.tab) {
-    int seg = 0;
-    for (int c = 0; c < D.nCtrl; ++c) seg |= (int)((rowBase >> D.ctrlShift[c]) & 1ull) << c;
-    const double2* tp = D.tab + ((size_t)seg << (LOGM + 1));
-    // T: permuted table, index r M + k2; S: natural, index (w / H) M + m_(w % H)
-    const double2* base = layoutT ? tp + r * M + t : tp + t + TPR * H * r;
-#pragma unroll
-    for (int k0 = 0; k0 < E; k0 += 8) {
-      double2 w[8];
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        const int kk = k0 + k;
-        w[k] = __ldg(base + (layoutT ? TPR * kk : (kk / H) * M + TPR * (kk % H)));
-      }
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        if (D.hasRowF) w[k] = dmul(w[k], rs);
-        v[k0 + k] = cmul(v[k0 + k], fromd<C>(w[k]));
-      }
-    }
-  } else if (D.hasRowF) {
-    const C c = fromd<C>(rs);
-#pragma unroll
-    for (int k = 0; k < E; ++k) v[k] = cmul(v[k], c);
-  }
-}
-
-// LOGE: log2 amplitudes per thread (16 for complex128: 512 threads, one CTA per
-// SM; 32 for complex64: 256 threads, two CTAs per SM)
-template <typename C, int LOGN, int LOGE>
-__global__ void __launch_bounds__(1 << (LOGN - 1 - LOGE), (LOGN - 1 - LOGE) > 8 ? 1 : 2)
-    k_rowc(const C* __restrict__ in, C* __restrict__ out, const __grid_constant__ RowProgram P) {
-  constexpr int LOGM = LOGN - 1, M = 1 << LOGM, E = 1 << LOGE, H = E / 2, TPR = M >> LOGE;
-  constexpr int RS = M + (M >> 4);
-  extern __shared__ __align__(16) unsigned char smraw[];
-  C* sm = reinterpret_cast<C*>(smraw);
-  double2* loM = reinterpret_cast<double2*>(sm + RS);  // w_M^e, e < 64
-  double2* hiM = loM + 64;                              // w_M^(64 h), h < M / 64
-  double2* loN = hiM + (M >> 6);                        // w_N^e, e < 64
-  double2* hiN = loN + 64;                              // w_N^(64 h), h < M / 64
-  cg::cluster_group cl = cg::this_cluster();
-  const int r = (int)cl.block_rank();
-  const int t = threadIdx.x;
-  const C* peer = cl.map_shared_rank(sm, r ^ 1);
-  const uint64_t rowBase = ((uint64_t)blockIdx.x >> 1) << LOGN;
-
-  {
-    const int scM = P.logTwN - LOGM, scN = P.logTwN - LOGN;
-    constexpr int NTAB = 2 * (64 + (M >> 6));
-    for (int i = t; i < NTAB; i += TPR) {
-      const int half = i >= NTAB / 2, j = half ? i - NTAB / 2 : i;
-      const int e = j < 64 ? j : (j - 64) << 6;
-      loM[i] = __ldg(P.tw + ((size_t)e << (half ? scN : scM)));  // loM..hiN are one array
-    }
-  }
-  C v[E];
-  bool layoutT = P.loadT != 0;
-  if (P.loadT == 2) {  // blocked: this CTA's X[r + 2 k2] are contiguous at r M + k2
-#pragma unroll
-    for (int w = 0; w < E; ++w) v[w] = in[rowBase + (uint64_t)r * M + t + TPR * w];
-  } else if (!layoutT) {
-    if (P.dualHead < 0) {
-#pragma unroll
-      for (int i = 0; i < H; ++i) {
-        v[i] = in[rowBase + t + TPR * (H * r + i)];
-        v[H + i] = in[rowBase + M + t + TPR * (H * r + i)];
-      }
-    }
-  } else {
-    // pairs X[2 k2], X[2 k2 + 1] for k2 in this CTA's half; keep X[r + 2 k2]
-    C keep[H], give[H], got[H];
-#pragma unroll
-    for (int i = 0; i < H; ++i) {
-      const uint64_t k2 = (uint64_t)(t + TPR * (H * r + i));
-      const C a = in[rowBase + 2 * k2], b = in[rowBase + 2 * k2 + 1];
-      keep[i] = r ? b : a;
-      give[i] = r ? a : b;
-    }
-    rc_swap<C, TPR, H>(sm, peer, t, give, got, r, r ^ 1);
-#pragma unroll
-    for (int i = 0; i < H; ++i) {
-      v[r ? H + i : i] = keep[i];
-      v[r ? i : H + i] = got[i];
-    }
-  }
-  __syncthreads();  // twiddle tables
-
-  int o0 = 0;
-  if (P.dualHead >= 0) {
-    // Leading forward transform: both CTAs read the whole row (the second read of
-    // each element comes from L2) and form y_r[m] = w_N^{m r} (x[m] + (-1)^r x[M + m])
-    // for all 16 of their m directly, after the leading diagonal runs.
-    double2 rs[2];
-    int seg[2];
-    for (int o = 0; o < P.dualHead; ++o) {
-      const RowDiag& D = P.diag[P.ops[o].diag];
-      rs[o] = D.hasRowF ? eval_factor(D.rowF, rowBase) : make_double2(1.0, 0.0);
-      int sg = 0;
-      for (int c = 0; c < D.nCtrl; ++c) sg |= (int)((rowBase >> D.ctrlShift[c]) & 1ull) << c;
-      seg[o] = sg << LOGN;
-    }
-#pragma unroll
-    for (int w0 = 0; w0 < E; w0 += 4) {
-      C a[4], b[4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int m = t + TPR * (w0 + j);
-        a[j] = in[rowBase + m];
-        b[j] = in[rowBase + M + m];
-      }
-      for (int o = 0; o < P.dualHead; ++o) {
-        const RowDiag& D = P.diag[P.ops[o].diag];
-        if (!D.tab && !D.hasRowF) continue;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int m = t + TPR * (w0 + j);
-          double2 fa = D.tab ? __ldg(D.tab + seg[o] + m) : make_double2(1.0, 0.0);
-          double2 fb = D.tab ? __ldg(D.tab + seg[o] + M + m) : make_double2(1.0, 0.0);
-          if (D.hasRowF) {
-            fa = dmul(fa, rs[o]);
-            fb = dmul(fb, rs[o]);
-          }
-          a[j] = cmul(a[j], fromd<C>(fa));
-          b[j] = cmul(b[j], fromd<C>(fb));
-        }
-      }
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int m = t + TPR * (w0 + j);
-        v[w0 + j] = r ? cmul(csub(a[j], b[j]), tw2<C, 1>(loN, hiN, m)) : cadd(a[j], b[j]);
-      }
-    }
-    rr_stages<C, 1, LOGM, 0, LOGE>(v, sm, t, loM, hiM);
-    layoutT = true;
-    o0 = P.dualHead + 1;
-  }
-
-  for (int o = o0; o < P.nOps; ++o) {
-    const RowOp& op = P.ops[o];
-    if (op.kind == kRowDiag) {
-      rc_diag<C, LOGM, LOGE>(v, P.diag[op.diag], rowBase, t, r, layoutT);
-    } else if (op.dir > 0) {  // S -> T
-      C mine[H], give[H], got[H];
-#pragma unroll
-      for (int i = 0; i < H; ++i) {
-        const int m = t + TPR * (H * r + i);
-        const C a = v[i], b = v[H + i];
-        const C y0 = cadd(a, b);
-        const C y1 = cmul(csub(a, b), tw2<C, 1>(loN, hiN, m));
-        mine[i] = r ? y1 : y0;
-        give[i] = r ? y0 : y1;
-      }
-      rc_swap<C, TPR, H>(sm, peer, t, give, got, r, r ^ 1);
-#pragma unroll
-      for (int i = 0; i < H; ++i) {
-        v[r ? H + i : i] = mine[i];
-        v[r ? i : H + i] = got[i];
-      }
-      rr_stages<C, 1, LOGM, 0, LOGE>(v, sm, t, loM, hiM);
-      layoutT = true;
-    } else {  // T -> S
-      rr_stages<C, -1, LOGM, 0, LOGE>(v, sm, t, loM, hiM);
-      C give[H], got[H];
-#pragma unroll
-      for (int i = 0; i < H; ++i) give[i] = v[r ? i : H + i];  // the sibling's half of z_r
-      rc_swap<C, TPR, H>(sm, peer, t, give, got, r ^ 1, r);
-#pragma unroll
-      for (int i = 0; i < H; ++i) {
-        const int m = t + TPR * (H * r + i);
-        const C z0 = r ? got[i] : v[i];
-        const C z1 = cmul(r ? v[H + i] : got[i], tw2<C, -1>(loN, hiN, m));
-        v[i] = cadd(z0, z1);
-        v[H + i] = csub(z0, z1);
-      }
-      layoutT = false;
-    }
-  }
-
-  if (!layoutT) {
-#pragma unroll
-    for (int i = 0; i < H; ++i) {
-      out[rowBase + t + TPR * (H * r + i)] = v[i];
-      out[rowBase + M + t + TPR * (H * r + i)] = v[H + i];
-    }
-  } else if (P.storeBlocked) {
-#pragma unroll
-    for (int w = 0; w < E; ++w) out[rowBase + (uint64_t)r * M + t + TPR * w] = v[w];
-  } else {
-    C give[H], got[H];
-#pragma unroll
-    for (int i = 0; i < H; ++i) give[i] = v[r ? i : H + i];  // X[r + 2 k2] for the sibling's k2
-    rc_swap<C, TPR, H>(sm, peer, t, give, got, r ^ 1, r);
-#pragma unroll
-    for (int i = 0; i < H; ++i) {
-      const uint64_t k2 = (uint64_t)(t + TPR * (H * r + i));
-      const C own = v[r ? H + i : i];
-      out[rowBase + 2 * k2] = r ? got[i] : own;
-      out[rowBase + 2 * k2 + 1] = r ? own : got[i];
-    }
-  }
-}
-
-template <typename C, int LOGN, int LOGE>
-static cudaError_t launch_rowc_t(Context* ctx, const RowProgram& P) {
-  constexpr int M = 1 << (LOGN - 1);
-  const size_t smem = (size_t)(M + (M >> 4)) * sizeof(C) + 2 * (64 + (M >> 6)) * sizeof(double2);
-  auto kern = k_rowc<C, LOGN, LOGE>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  cudaLaunchConfig_t cfg{};
-  cfg.gridDim = dim3((unsigned)(ctx->size() >> (LOGN - 1)));
-  cfg.blockDim = dim3(M >> LOGE);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = ctx->stream;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = 2;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, kern, (const C*)ctx->state(), (C*)ctx->other(), P);
 }
 
 // ---------------------------------------------------------------- four-CTA register-resident rows
@@ -1323,9 +1059,9 @@ static cudaError_t launch_row_t(Context* ctx, const RowProgram& P, uint64_t nCta
   return cudaLaunchKernelEx(&cfg, kern, (const C*)ctx->state(), (C*)ctx->other(), P);
 }
 
-// 2^14-point complex128 rows run on the two-CTA kernel.  (Complex64 rows of that
-// length fit one CTA, k_rowr; the two-CTA form with two 256-thread CTAs per SM
-// measured slower for them: the half swaps cost more than the overlap gains.)
+// 2^14-point complex128 rows run on the four-CTA kernel (k_rowq).  Complex64 rows
+// of that length fit one CTA, k_rowr, which measured faster for them than k_rowq
+// (2.0 against 1.5 ms per 2^28-amplitude launch).
 static bool rowc_shape(Context* ctx, int reg, const std::vector<HostRowOp>& ops) {
   if (ctx->precision != kC128 || ctx->q[reg] != 14 || !row_eligible(ctx, reg)) return false;
   int lastDir = 0;
@@ -1337,16 +1073,9 @@ static bool rowc_shape(Context* ctx, int reg, const std::vector<HostRowOp>& ops)
   return true;
 }
 
-// log2 of the cluster that runs 2^14-point complex128 row programs: 2 (k_rowq,
-// four 256-thread CTAs) or, with CVDV_ROW_CLUSTER=2 in the environment, 1 (k_rowc,
-// two 512-thread CTAs); the blocked layout between paired programs follows it.
-int rowc_log_cluster() {
-  static const int lc = [] {
-    const char* e = getenv("CVDV_ROW_CLUSTER");
-    return (e && atoi(e) == 2) ? 1 : 2;
-  }();
-  return lc;
-}
+// log2 of the cluster that runs 2^14-point complex128 row programs (k_rowq: four
+// 256-thread CTAs); the blocked layout between paired programs follows it.
+int rowc_log_cluster() { return 2; }
 
 bool rowc_takes(Context* ctx, int reg, const std::vector<HostRowOp>& ops) {
   if (!rowc_shape(ctx, reg, ops)) return false;
@@ -1479,10 +1208,10 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
   bool elemF = false;
   for (int d = 0; d < P.nDiag; ++d) elemF |= P.diag[d].hasElemF != 0;
   if ((blockedIn || blockedOut) && !useC) {
-    set_error(ctx, kErrUnsupported, "blocked layout requested for a program the two-CTA kernel does not run");
+    set_error(ctx, kErrUnsupported, "blocked layout requested for a program the four-CTA kernel does not run");
     return false;
   }
-  // the two-CTA kernel needs transforms that alternate in direction (each forward
+  // the four-CTA kernel needs transforms that alternate in direction (each forward
   // leaves the transposed layout an inverse consumes)
   bool alternating = true;
   int lastDir = 0;
@@ -1494,16 +1223,10 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
   if (useC && !elemF && alternating) {
     if (blockedIn) P.loadT = 2;
     P.storeBlocked = blockedOut ? 1 : 0;
-    P.dualHead = -1;
-    if (P.loadT == 0 && logC == 1) {
-      int f = 0;
-      while (f < P.nOps && P.ops[f].kind == kRowDiag) ++f;
-      if (f < P.nOps && f <= 2 && P.ops[f].dir > 0) P.dualHead = f;
-    }
     cudaError_t er;
     {
       LaunchScope _ls(ctx, kKFft);
-      er = logC == 2 ? launch_rowq_t<double2, 14>(ctx, P) : launch_rowc_t<double2, 14, 4>(ctx, P);
+      er = launch_rowq_t<double2, 14>(ctx, P);
     }
     if (!cuda_ok(ctx, er, "row program launch")) return false;
     ctx->cur ^= 1;

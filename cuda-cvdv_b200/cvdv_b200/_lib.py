@@ -86,7 +86,7 @@ SIGNATURES = [
     ("cvdvGetKernelStats", [c_void_p, POINTER(c_double), POINTER(ctypes.c_longlong), c_int], c_int),
 ]
 
-KERNEL_KINDS = ["fft_pass", "pair", "diag", "perm", "table", "init", "reduce", "phase_space", "seq", "col"]
+KERNEL_KINDS = ["fft_pass", "pair", "diag", "perm", "table", "init", "reduce", "phase_space", "seq", "col", "col_tc"]
 
 
 def kernel_stats(ctx):

@@ -61,7 +61,9 @@ class CudaCvdv:
         as one pass with each column on chip; bit 4 applies the gates queued
         after initStateVector that act on one mode alone (before it is coupled
         to another register) to that mode's array before the product state is
-        formed.  True = all, False = none, an int = those bits."""
+        formed; bit 5 (not in True; opt-in) runs complex64 transforms of non-last
+        registers of 2^12 .. 2^14 points as DFT-matrix products on the tensor
+        cores.  True = bits 0-4, False = none, an int = those bits."""
         flags = (31 if on else 0) if isinstance(on, bool) else int(on)
         self._L.cvdvSetFusion(self.ctx, flags)
 

@@ -170,7 +170,12 @@ void* cvdvGetStream(CVDVContext* ctx);
  * cvdvInitFromSeparable on two or more registers, the queued stages that act on
  * one register of 2^8 .. 2^14 points alone, ahead of every stage that couples it
  * to another register, run on that register's array before the product is formed
- * (at the next flush).  cvdvCancelledTransforms counts the transforms removed so
+ * (at the next flush).  flags bit 5 (default off): in complex64 contexts, the
+ * transforms of a register that is not the last one, of 2^12 .. 2^14 points with
+ * at least 32 amplitudes below it, run their two-pass (chained) column passes as
+ * DFT-matrix products on the tensor cores (split-BF16 three-term products, FP32
+ * accumulation, about 3e-6 relative error per 128-point DFT) instead of bit 3's
+ * one-pass programs.  cvdvCancelledTransforms counts the transforms removed so
  * far. */
 void cvdvSetFusion(CVDVContext* ctx, int flags);
 long long cvdvCancelledTransforms(CVDVContext* ctx);
