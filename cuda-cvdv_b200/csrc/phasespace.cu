@@ -22,6 +22,7 @@
 
 #include "../../include/cvdv.h"
 #include "cvdv_internal.cuh"
+#include "row_fft.cuh"
 
 using namespace cvdv;
 struct CVDVContext : public cvdv::Context {};
@@ -261,6 +262,93 @@ __global__ void k_husimi_gauss2d(double2* __restrict__ spec, int N, double dx) {
   }
 }
 
+// G[k] once per readout
+__global__ void k_husimi_g(int N, double dx, double* __restrict__ G) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) G[k] = husimi_g(k, N, dx);
+}
+
+// The overlap route in one pass per output row.  Row m of the result is
+//   Q[(m + N/2) mod N][q] = 1/(pi N^2) sum_s |H_s[q]|^2,  H_s = IDFT_k( Psi_s[(m + k) mod N] G[k] ),
+// so a thread group of N/16 threads forms A_s[k] for its 16 points k = t + (N/16) e
+// straight from the transformed slices Psi (S N values, read from L2 for every m),
+// runs the inverse N-point DFT in registers (the row kernels' Stockham stages,
+// one padded shared-memory row), adds |H_s|^2 to its 16 accumulators, and after
+// the last slice writes its part of the output row.  The S N^2 circulant the
+// reference materialises (bosonic.cu:10-61, bosonic.cuh:112-150) is never stored,
+// and no atomics or separate accumulation and finalisation passes are needed.
+template <int LOGN>
+__global__ void __launch_bounds__((1 << (LOGN - 4)) > 256 ? (1 << (LOGN - 4)) : 256)
+    k_husimi_rows(const double2* __restrict__ Psi, const double* __restrict__ G, uint64_t S,
+                  const double2* __restrict__ tw, int logTwN, double* __restrict__ out) {
+  constexpr int N = 1 << LOGN, E = 16, TPR = N / E;
+  constexpr int ROWS = TPR >= 256 ? 1 : (256 / TPR < N ? 256 / TPR : N);  // output rows per CTA
+  constexpr int RS = N + (N >> 4);
+  constexpr int NHI = N >= 64 ? N / 64 : 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double2* sm = reinterpret_cast<double2*>(smraw);
+  double2* lo = sm + ROWS * RS;  // w_N^e, e < 64
+  double2* hi = lo + 64;         // w_N^(64 h), h < N / 64
+  const int tid = threadIdx.x, row = tid / TPR, t = tid % TPR;
+  for (int i = tid; i < 64 + NHI; i += TPR * ROWS) {
+    const int e = i < 64 ? i : (i - 64) << 6;
+    lo[i] = e < N ? __ldg(tw + ((size_t)e << (logTwN - LOGN))) : make_double2(1.0, 0.0);
+  }
+  __syncthreads();
+  const int m = blockIdx.x * ROWS + row;
+  double2* smrow = sm + row * RS;
+  double g[E], acc[E];
+#pragma unroll
+  for (int k = 0; k < E; ++k) {
+    g[k] = __ldg(G + t + TPR * k);
+    acc[k] = 0.0;
+  }
+  for (uint64_t s = 0; s < S; ++s) {
+    const double2* ps = Psi + s * N;
+    double2 v[E];
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+      const double2 p = __ldg(ps + ((m + t + TPR * k) & (N - 1)));
+      v[k] = make_double2(p.x * g[k], p.y * g[k]);
+    }
+    rr_stages<double2, -1, LOGN, 0, 4>(v, smrow, t, lo, hi);  // v[k] = H_s[t + TPR k]
+#pragma unroll
+    for (int k = 0; k < E; ++k) acc[k] += v[k].x * v[k].x + v[k].y * v[k].y;
+  }
+  const double norm = 1.0 / (CVDV_PI * (double)N * (double)N);
+  double* o = out + (size_t)((m + N / 2) & (N - 1)) * N;
+#pragma unroll
+  for (int k = 0; k < E; ++k) o[t + TPR * k] = acc[k] * norm;
+}
+
+template <int LOGN>
+static cudaError_t husimi_rows_t(Context* c, const double2* Psi, const double* G, uint64_t S, double* out) {
+  constexpr int N = 1 << LOGN, TPR = N / 16, ROWS = TPR >= 256 ? 1 : (256 / TPR < N ? 256 / TPR : N);
+  const size_t smem = (size_t)ROWS * (N + (N >> 4)) * sizeof(double2) + (64 + (N >= 64 ? N / 64 : 1)) * sizeof(double2);
+  auto kern = k_husimi_rows<LOGN>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int logTwN = 0;
+  while ((1 << logTwN) < c->twN) ++logTwN;
+  kern<<<N / ROWS, TPR * ROWS, smem, c->stream>>>(Psi, G, S, c->twiddle, logTwN, out);
+  return cudaGetLastError();
+}
+
+static cudaError_t husimi_rows(Context* c, int q, const double2* Psi, const double* G, uint64_t S, double* out) {
+  switch (q) {
+    case 4: return husimi_rows_t<4>(c, Psi, G, S, out);
+    case 5: return husimi_rows_t<5>(c, Psi, G, S, out);
+    case 6: return husimi_rows_t<6>(c, Psi, G, S, out);
+    case 7: return husimi_rows_t<7>(c, Psi, G, S, out);
+    case 8: return husimi_rows_t<8>(c, Psi, G, S, out);
+    case 9: return husimi_rows_t<9>(c, Psi, G, S, out);
+    case 10: return husimi_rows_t<10>(c, Psi, G, S, out);
+    case 11: return husimi_rows_t<11>(c, Psi, G, S, out);
+    case 12: return husimi_rows_t<12>(c, Psi, G, S, out);
+    case 13: return husimi_rows_t<13>(c, Psi, G, S, out);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 // max(Re / N^2, 0)   (kernelComplexToRealNormalizedClamp, bosonic.cuh:180-186)
 __global__ void k_real_clamp(const double2* __restrict__ in, uint64_t NN, double norm,
                              double* __restrict__ out) {
@@ -372,6 +460,43 @@ static void husimi_overlap_route(Context* c, int r, double* husimiOut) {
   int N = 1 << q;
   uint64_t S = c->size() >> q;
   size_t NN = (size_t)N * N;
+  if (q >= 4 && q <= 13) {
+    // slices, their transforms and the transform's scratch (3 S N), G (N), the output (N^2)
+    char* work = (char*)big_scratch(c, (3 * S * N) * sizeof(double2) + (N + NN) * sizeof(double));
+    if (!work) return;
+    double2* X = (double2*)work;
+    double2* Psi = X + S * N;
+    double2* T = Psi + S * N;
+    double* G = (double*)(T + S * N);
+    double* dOut = G + N;
+    {
+      LaunchScope _ls(c, kKPhaseSpace);
+      if (c->precision == kC128)
+        k_extract_slices<double2><<<gblocks(S * N), 256, 0, c->stream>>>((const double2*)c->state(), N, q, flw, 0, S, X);
+      else
+        k_extract_slices<float2><<<gblocks(S * N), 256, 0, c->stream>>>((const float2*)c->state(), N, q, flw, 0, S, X);
+    }
+    if (!launch_fft_generic(c, X, Psi, T, S, q, 1, 1, kC128)) {
+      set_error(c, kErrUnsupported, "husimi: register too large");
+      return;
+    }
+    {
+      LaunchScope _ls(c, kKPhaseSpace);
+      k_husimi_g<<<gblocks(N), 256, 0, c->stream>>>(N, c->dx[r], G);
+    }
+    cudaError_t e;
+    {
+      LaunchScope _ls(c, kKPhaseSpace);
+      e = husimi_rows(c, q, Psi, G, S, dOut);
+    }
+    if (!cuda_ok(c, e, "husimi launch")) return;
+    if (!cuda_ok(c, cudaMemcpyAsync(husimiOut, dOut, NN * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
+                 "husimi copy"))
+      return;
+    stream_sync(c, "husimi sync");
+    return;
+  }
+  // longer registers: the circulant in chunks of slices, transformed by the pass kernel
   // slices per chunk: the circulant A of a chunk holds cs * N^2 complex values
   uint64_t cs = ((uint64_t)1 << 25) / NN;
   if (cs < 1) cs = 1;

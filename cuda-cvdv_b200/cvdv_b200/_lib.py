@@ -69,6 +69,7 @@ SIGNATURES = [
     ("cvdvGetStateDevicePtr", [c_void_p], c_void_p),
     ("cvdvGetStream", [c_void_p], c_void_p),
     ("cvdvMeasureEach", [c_void_p, POINTER(c_int), c_int, POINTER(c_double)], None),
+    ("cvdvSeparableFill", [c_void_p, c_int, c_int, POINTER(c_double), c_int, c_void_p], c_int),
     ("cvdvMeasureMultipleNoAlloc",
      [c_void_p, c_int, POINTER(c_int), c_int, POINTER(c_int), c_int, c_void_p, c_void_p], c_int),
     ("cvdvBatchRx", [c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_double, c_void_p], c_int),

@@ -265,6 +265,17 @@ void cvdvBatchStructSizes(int* sizes);
 int cvdvBatchRunStage(void* states, int precision, const CvdvBatchTask* tasks, int nTasks,
                       const CvdvBatchProgram* programs, int gridCtas, void* stream);
 
+/* Device-side separable register arrays (the input of cvdvInitFromSeparable), the
+ * generators of src/cvdv.cu:187-295 and the setters of src/separable.py:44-132:
+ * writes 2^numQubits complex128 values to the device array `out` on `stream`
+ * (NULL = default stream), enqueue only.  kind / params:
+ *   0 basis state {j0}; 1 uniform {}; 2 coherent {Re a, Im a};
+ *   3 Fock {n}; 4 Fock superposition {Re c0, Im c0, Re c1, Im c1, ...};
+ *   5 normalised sum of coherent states {Re a, Im a, Re c, Im c, ...};
+ *   6 squeezed coherent D(a) S(r)|0> {r, Re a, Im a} (no reference setter).
+ * At most 256 parameters.  Returns 0 or an error code (cvdvGetLastError(NULL, ..)). */
+int cvdvSeparableFill(void* out, int numQubits, int kind, const double* params, int nParams, void* stream);
+
 /* No counterpart in the reference.  The joint marginal of cvdvMeasureMultiple
  * for callers that cannot let the library allocate device memory (their device
  * memory belongs to another allocator, is fixed at start-up, or must not see

@@ -144,6 +144,23 @@ def test_husimi_overlap_alias():
         np.testing.assert_allclose(out.reshape(N, N), sim.getHusimiQ(reg), atol=1e-14)
 
 
+@pytest.mark.parametrize("qubits,reg", [([1, 12], 1), ([12, 2], 0), ([2, 9, 3], 1)])
+def test_husimi_overlap_rows(qubits, reg):
+    """The overlap route's fused row kernel (the circulant formed on the fly, one
+    pass per output row) against the oracle's restatement of the reference's route,
+    up to N = 4096 and on a strided register."""
+    rng = np.random.default_rng(sum(qubits) + reg)
+    n = sum(qubits)
+    psi = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    psi /= np.linalg.norm(psi)
+    sim = make(qubits, psi)
+    o = oracle(qubits, psi)
+    ref = o.husimi(reg)
+    got = sim.getHusimiQ(reg)
+    assert np.abs(got - ref).max() < 1e-12 * max(1.0, np.abs(ref).max())
+    np.testing.assert_allclose(make(qubits, psi, "complex64").getHusimiQ(reg), ref, atol=2e-5 * np.abs(ref).max())
+
+
 def test_large_marginal_global_path():
     """> 4096 bins uses the global-atomic path."""
     rng = np.random.default_rng(5)
@@ -765,3 +782,44 @@ def test_mode_bits_between_paired_transforms():
             sim = make(qubits, psi, prec)
             run(sim, seq)
             assert rel(sim.getState(), ref) < tol, (prec, seq)
+
+
+def test_device_separable_setters_match_reference_fixtures():
+    """SeparableState on a CUDA device writes the register arrays with the
+    generator kernel (cvdvSeparableFill); they equal the reference setters'
+    output (tests/golden/separable.npz, generated by src/separable.py)."""
+    from cvdv_b200 import SeparableState
+    SEP = dict(np.load(os.path.join(GOLD, "separable.npz")))
+    for nq in (3, 6, 10):
+        sep = SeparableState([nq], device="cuda")
+        checks = [("zero", lambda: sep.setZero(0)), ("uniform", lambda: sep.setUniform(0))]
+        checks += [(f"coherent_{a}", (lambda a=a: sep.setCoherent(0, a))) for a in (0.0, 1.0, 1.5 + 0.8j, -0.5 + 2.0j)]
+        checks += [(f"fock_{n}", (lambda n=n: sep.setFock(0, n))) for n in (0, 1, 2, 5)]
+        checks += [("focks", lambda: sep.setFocks(0, [0.6, 0.8j, 0.0])),
+                   ("cat", lambda: sep.setCat(0, [(2.0, 1.0), (-2.0, 1.0)]))]
+        for name, setter in checks:
+            setter()
+            a = sep.register_arrays[0]
+            assert a.is_cuda and a.dtype == torch.complex128
+            key = name.replace("_", f"_{nq}_", 1) if "_" in name else f"{name}_{nq}"
+            np.testing.assert_allclose(a.cpu().numpy(), SEP[key], atol=1e-14, err_msg=key)
+
+
+@pytest.mark.parametrize("q,rr,alpha", [(10, 0.3, 0.0), (10, 0.3, 1.2 - 0.7j), (12, -0.4, 0.5 + 0.3j),
+                                        (14, 0.45, -1.1 + 0.9j)])
+def test_squeezed_setter_matches_gates(q, rr, alpha):
+    """setSqueezed(r, a) is the state the squeeze and displacement gates make
+    from the vacuum (setFock(0), s(r), d(a)), on the device and on the host."""
+    from cvdv_b200 import CudaCvdv, SeparableState
+    ref = SeparableState([q], device="cuda")
+    ref.setFock(0, 0)
+    sim = CudaCvdv([q], check_errors=True)
+    sim.initStateVector(ref)
+    sim.s(0, rr)
+    sim.d(0, alpha)
+    want = sim.getState()
+    for dev in ("cuda", "cpu"):
+        sep = SeparableState([q], device=dev)
+        sep.setSqueezed(0, rr, alpha)
+        got = sep.register_arrays[0].cpu().numpy()
+        assert rel(got, want) < 1e-10, (dev, rel(got, want))

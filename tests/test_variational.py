@@ -79,6 +79,38 @@ def test_adjoint_matches_central_differences():
     assert np.abs(grad - fd).max() < 1e-6 * scale + 1e-9, np.abs(grad - fd).max() / scale
 
 
+def _central_differences(circ, params, psi0, tgt, h=1e-4):
+    """Central differences of the loss for every parameter of every set: all
+    2 x sets x params perturbed sets in one batched forward of `circ`."""
+    B, P = params.shape
+    plus = params.repeat_interleave(P, dim=0)
+    minus = plus.clone()
+    idx = torch.arange(P).repeat(B)
+    plus[torch.arange(plus.shape[0]), idx] += h
+    minus[torch.arange(minus.shape[0]), idx] -= h
+    with torch.no_grad():
+        lp = circ.fidelity_loss(plus, psi0, tgt).cpu().numpy()
+        lm = circ.fidelity_loss(minus, psi0, tgt).cpu().numpy()
+    return ((lp - lm) / (2 * h)).reshape(B, P)
+
+
+def test_full_config_adjoint_matches_central_differences():
+    """The configured problem: 64 parameter sets of [1, 12], 40 layers (80 gates),
+    checkpoints every 8 layers.  The complex128 adjoint against central differences
+    (h = 1e-4) of the complex128 forward: max error within 1e-6 of the largest
+    gradient; the complex64 adjoint within 1e-3 of it."""
+    w, params, psi0, tgt = _problem(batch=64, layers=40, mode_qubits=12)
+    fd = _central_differences(_circ("complex128", 40, 12, checkpoint_every=16), params, psi0, tgt)
+    scale = np.abs(fd).max()
+    assert scale > 1e-3
+    for precision, tol in (("complex128", 1e-6), ("complex64", 1e-3)):
+        circ = _circ(precision, 40, 12, checkpoint_every=16)
+        p = params.clone().requires_grad_(True)
+        circ.fidelity_loss(p, psi0, tgt).sum().backward()
+        err = np.abs(p.grad.numpy() - fd).max() / scale
+        assert err < tol, (precision, err)
+
+
 def _torch_forward(params, psi0, layers, mq):
     """Differentiable complex128 restatement: Rx on the qubit, cd = FtP2Q exp(i beta K) FtQ2P."""
     N = 1 << mq
