@@ -467,7 +467,11 @@ def batched_c4(args):
     from cvdv_b200.batch import BatchedCircuits, random_instances
     insts = random_instances(seed=4, count=512, gates=50)
     B = BatchedCircuits(insts, precision="complex64")
-    grid, chunk = B.autotune(reps=1)
+    # the default shapes, then the autotuned ones (grid, pair chunk, row-task shape per mode length)
+    psi_tmp = [W.product_state(i["qubits"], i["init"]) for i in insts]
+    B.set_initial(psi_tmp)
+    ms_default = B._time(3)
+    grid, chunk = B.autotune(reps=2)
     psi0 = [W.product_state(i["qubits"], i["init"]) for i in insts]
     B.set_initial(psi0)
     B.run(graph=True)  # one run + capture
@@ -496,6 +500,9 @@ def batched_c4(args):
     return {"value": len(insts) / (ms * 1e-3), "unit": "instances/s", "ms_per_run": ms,
             "instances": len(insts), "gates_per_instance": 50, "amplitudes": amps,
             "state_bytes": amps * 8, "gpu_launches_per_run": B.n_stages, "grid": grid, "pair_chunk": chunk,
+            "row_loge": {str(k): v for k, v in sorted(B.row_loge.items())},
+            "ms_per_run_default_shapes": ms_default,
+            "autotune_trials": {"grid_chunk": B.tuning["grid_chunk"], "row_loge": B.tuning["row_loge"]},
             "per_instance_loop": {"value": loop_n / loop_s, "unit": "instances/s", "instances": loop_n,
                                   "how": "CudaCvdv complex64, one instance after another, wall clock"},
             "speedup_vs_loop": (len(insts) / (ms * 1e-3)) / (loop_n / loop_s),

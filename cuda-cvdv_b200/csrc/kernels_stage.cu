@@ -25,19 +25,24 @@ namespace cvdv {
 
 constexpr int kStageThreads = 512;
 
-// amplitudes per thread: 32 for complex64 rows of 2^13 and 2^14 points, else 16
-// (complex128 rows stop at 2^13 points: 512 threads x 16)
-template <typename C, int LOGN>
-struct StageShape {
-  static constexpr int LOGE = (sizeof(C) == sizeof(float2) && LOGN >= 13) ? 5 : 4;
-};
+// Amplitudes per thread of a row task, 2^LOGE with LOGE = 3, 4 or 5 (radix-8, 16 or
+// 32 Stockham stages; 512 2^LOGE / N rows per CTA), chosen per task (the
+// autotuner's knob).  A row must fit the 512 threads (N / 2^LOGE <= 512) and the
+// CTA's rows the shared memory (complex128: 2^LOGE <= 16).  The default is 32 for
+// complex64 rows of 2^13 and 2^14 points, else 16.
 template <typename C> constexpr int stage_max_log() { return sizeof(C) == sizeof(float2) ? 14 : 13; }
+template <typename C> constexpr int stage_max_loge() { return sizeof(C) == sizeof(float2) ? 5 : 4; }
+template <typename C, int LOGN, int LOGE>
+constexpr bool stage_shape_ok() {
+  return LOGE >= 3 && LOGE <= stage_max_loge<C>() && LOGN >= LOGE && (LOGN - LOGE) <= 9;
+}
 
-// shared memory of the largest row group (512 threads x E amplitudes, padded) + twiddles
+// shared memory of the largest row group (512 threads x E amplitudes, padded) + twiddles;
+// the radix-8 shape's rows (512 x 8 amplitudes, padded by 1/8) are smaller
 template <typename C>
 constexpr size_t stage_smem() {
   constexpr int L = stage_max_log<C>();
-  constexpr int E = 1 << StageShape<C, L>::LOGE;
+  constexpr int E = 1 << stage_max_loge<C>();
   return (size_t)(kStageThreads * E + kStageThreads * E / 16) * sizeof(C) + (64 + (1 << (L - 6))) * sizeof(double2);
 }
 
@@ -68,12 +73,13 @@ __device__ __forceinline__ C phase_factor(const CvdvBatchPhase& P, int j, int N,
   return mk(sc * c, sc * s);
 }
 
-template <typename C, int LOGN>
+template <typename C, int LOGN, int LOGE>
 __device__ __forceinline__ void stage_row_task(C* __restrict__ st, const CvdvBatchTask& T,
                                                const CvdvBatchProgram& Pg, unsigned char* smraw) {
-  constexpr int LOGE = StageShape<C, LOGN>::LOGE;
   constexpr int E = 1 << LOGE, N = 1 << LOGN, TPR = N >> LOGE, R = kStageThreads / TPR;
-  constexpr int RS = N + (N >> 4);
+  // the Stockham exchanges pad a row once per radix: every 8 points for radix-8
+  // stages (LOGE 3), every 16 or 32 otherwise
+  constexpr int RS = N + (N >> (LOGE == 3 ? 3 : 4));
   C* sm = reinterpret_cast<C*>(smraw);
   double2* lo = reinterpret_cast<double2*>(sm + (size_t)RS * R);
   double2* hi = lo + 64;
@@ -128,6 +134,19 @@ __device__ __forceinline__ void stage_row_task(C* __restrict__ st, const CvdvBat
   __syncthreads();  // shared memory is reused by the CTA's next task
 }
 
+template <typename C, int LOGN>
+__device__ __forceinline__ void stage_row_dispatch(C* __restrict__ st, const CvdvBatchTask& T,
+                                                   const CvdvBatchProgram& Pg, unsigned char* smraw, int le) {
+  // (the host checks every task's shape against stage_shape_ok before launching)
+  if (le == 3) {
+    if constexpr (stage_shape_ok<C, LOGN, 3>()) stage_row_task<C, LOGN, 3>(st, T, Pg, smraw);
+  } else if (le == 4) {
+    if constexpr (stage_shape_ok<C, LOGN, 4>()) stage_row_task<C, LOGN, 4>(st, T, Pg, smraw);
+  } else {
+    if constexpr (stage_shape_ok<C, LOGN, 5>()) stage_row_task<C, LOGN, 5>(st, T, Pg, smraw);
+  }
+}
+
 template <typename C>
 __device__ __forceinline__ void stage_pair_task(C* __restrict__ st, const CvdvBatchTask& T) {
   const C a00 = fromd<C>(make_double2(T.m[0], T.m[1])), a01 = fromd<C>(make_double2(T.m[2], T.m[3]));
@@ -156,15 +175,16 @@ __global__ void __launch_bounds__(kStageThreads, 1)
       continue;
     }
     const CvdvBatchProgram& Pg = progs[T.program];
+    const int le = T.logE ? T.logE : ((sizeof(C) == sizeof(float2) && T.logRow >= 13) ? 5 : 4);
     switch (T.logRow) {
-      case 8: stage_row_task<C, 8>(st, T, Pg, smraw); break;
-      case 9: stage_row_task<C, 9>(st, T, Pg, smraw); break;
-      case 10: stage_row_task<C, 10>(st, T, Pg, smraw); break;
-      case 11: stage_row_task<C, 11>(st, T, Pg, smraw); break;
-      case 12: stage_row_task<C, 12>(st, T, Pg, smraw); break;
-      case 13: stage_row_task<C, 13>(st, T, Pg, smraw); break;
+      case 8: stage_row_dispatch<C, 8>(st, T, Pg, smraw, le); break;
+      case 9: stage_row_dispatch<C, 9>(st, T, Pg, smraw, le); break;
+      case 10: stage_row_dispatch<C, 10>(st, T, Pg, smraw, le); break;
+      case 11: stage_row_dispatch<C, 11>(st, T, Pg, smraw, le); break;
+      case 12: stage_row_dispatch<C, 12>(st, T, Pg, smraw, le); break;
+      case 13: stage_row_dispatch<C, 13>(st, T, Pg, smraw, le); break;
       default:
-        if constexpr (stage_max_log<C>() >= 14) stage_row_task<C, 14>(st, T, Pg, smraw);
+        if constexpr (stage_max_log<C>() >= 14) stage_row_dispatch<C, 14>(st, T, Pg, smraw, le);
         break;
     }
   }

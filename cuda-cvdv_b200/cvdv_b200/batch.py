@@ -15,8 +15,13 @@ follow the single-instance path exactly (thresholds 1e-12 / 1e-15, rint for the
 rotation's quarter turns, dropped global phases), so every instance matches
 ``CudaCvdv`` running the same gates.
 
-Tuning: the persistent grid size and the pair-gate chunk are picked by
-``autotune()`` (timed candidates on the compiled batch).
+Tuning: ``autotune()`` times candidates on the compiled batch: the persistent
+grid size, the pair-gate chunk (the 2x2-gate tasks' shape), and, per mode
+length 2^m of the batch, the row tasks' amplitudes per thread 2^logE -- which
+is both the radix schedule of their transforms (radix-8, 16 or 32 Stockham
+stages) and the rows a CTA holds (512 2^logE / 2^m) -- by coordinate descent
+over the mode lengths, largest total work first.  The result is kept per
+(mode length, precision) in ``row_loge``.
 """
 
 from __future__ import annotations
@@ -35,11 +40,22 @@ PHASE_DTYPE = np.dtype([("a1", "f8"), ("b1", "f8"), ("a2", "f8"), ("b2", "f8"), 
                         ("h0", "f8"), ("scale", "f8"), ("tw", "i4"), ("ctrlBit", "i4")])
 PROGRAM_DTYPE = np.dtype([("nOps", "i4"), ("op", "i4", (15,)), ("phase", PHASE_DTYPE, (8,))])
 TASK_DTYPE = np.dtype([("stateOffset", "i8"), ("kind", "i4"), ("n", "i4"), ("logRow", "i4"), ("first", "i4"),
-                       ("count", "i4"), ("bit", "i4"), ("program", "i4"), ("pad", "i4"), ("m", "f8", (8,))])
+                       ("count", "i4"), ("bit", "i4"), ("program", "i4"), ("logE", "i4"), ("m", "f8", (8,))])
 
 OP_DIAG, OP_FWD, OP_INV, OP_PARITY = 0, 1, 2, 3
 SQRT2 = math.sqrt(2.0)
 THREADS = 512
+
+
+def loge_options(m: int, prec: int) -> List[int]:
+    """Amplitudes per thread (log2) a row task of 2^m points can use: a row fits the
+    512 threads, and complex128 rows at most 16 per thread (shared memory)."""
+    top = 5 if prec == 1 else 4
+    return [e for e in (3, 4, 5) if e <= top and e <= m and m - e <= 9]
+
+
+def default_loge(m: int, prec: int) -> int:
+    return 5 if (prec == 1 and m >= 13) else 4
 
 
 def struct_sizes() -> Tuple[int, int, int]:
@@ -200,13 +216,19 @@ class BatchedCircuits:
     QUBIT_GATES = ("h", "rx", "ry", "rz")
 
     def __init__(self, instances: Sequence[Dict[str, Any]], precision: str = "complex64",
-                 pair_chunk: int = 4096, grid: int = 148) -> None:
-        """instances: dicts with ``qubits`` ([1]*Q + [m]) and ``gates`` [(name, args)]."""
+                 pair_chunk: int = 4096, grid: int = 148, row_loge: Optional[Dict[int, int]] = None) -> None:
+        """instances: dicts with ``qubits`` ([1]*Q + [m]) and ``gates`` [(name, args)];
+        row_loge: amplitudes per thread (log2) of the row tasks per mode length m
+        (default 4, or 5 for complex64 modes of 2^13 and 2^14 points)."""
         self.prec = PRECISIONS[precision]
         self.cdtype = torch.complex128 if self.prec == 0 else torch.complex64
         self.instances = list(instances)
         self.grid = grid
         self.pair_chunk = pair_chunk
+        self.row_loge: Dict[int, int] = dict(row_loge or {})
+        for m, e in self.row_loge.items():
+            if e not in loge_options(m, self.prec):
+                raise ValueError(f"row_loge[{m}] = {e}: choose from {loge_options(m, self.prec)}")
         max_log = 14 if self.prec == 1 else 13
         self.offsets = []
         off = 0
@@ -231,8 +253,8 @@ class BatchedCircuits:
             q = inst["qubits"]
             n, m = sum(q), q[-1]
             mode = len(q) - 1
-            E = 32 if (self.prec == 1 and m >= 13) else 16
-            rows_per_task = max(1, THREADS // ((1 << m) // E))
+            logE = self.row_loge.get(m, default_loge(m, self.prec))
+            rows_per_task = max(1, THREADS // ((1 << m) >> logE))
             for s, (name, args) in enumerate(inst["gates"]):
                 if name in self.QUBIT_GATES:
                     reg = args[0]
@@ -243,7 +265,7 @@ class BatchedCircuits:
                         ph = P._diag()
                         ph.ctrl = bit
                         ph.c["h0"] = -0.5 * float(args[-1])
-                        stage_tasks[s] += self._row_tasks(i, n, m, len(progs), rows_per_task)
+                        stage_tasks[s] += self._row_tasks(i, n, m, len(progs), rows_per_task, logE)
                         progs.append(P.record())
                     else:
                         pairs = 1 << (n - 1)
@@ -263,7 +285,7 @@ class BatchedCircuits:
                     else:
                         args = tuple(args[1:])
                     P = _mode_program(name, args, 1 << m, ctrl)
-                    stage_tasks[s] += self._row_tasks(i, n, m, len(progs), rows_per_task)
+                    stage_tasks[s] += self._row_tasks(i, n, m, len(progs), rows_per_task, logE)
                     progs.append(P.record())
         self.n_programs = len(progs)
         prog_arr = np.array(progs, dtype=PROGRAM_DTYPE) if progs else np.zeros(1, dtype=PROGRAM_DTYPE)
@@ -286,13 +308,13 @@ class BatchedCircuits:
             self._validate(arr)
             self._tasks.append((torch.from_numpy(arr.view(np.uint8).copy()).cuda(), len(arr)))
 
-    def _row_tasks(self, i: int, n: int, m: int, prog: int, per: int) -> List[np.void]:
+    def _row_tasks(self, i: int, n: int, m: int, prog: int, per: int, logE: int) -> List[np.void]:
         out = []
         rows = 1 << (n - m)
         for first in range(0, rows, per):
             t = np.zeros((), dtype=TASK_DTYPE)
             t["stateOffset"], t["kind"], t["n"], t["logRow"] = self.offsets[i], 0, n, m
-            t["first"], t["count"], t["program"] = first, min(per, rows - first), prog
+            t["first"], t["count"], t["program"], t["logE"] = first, min(per, rows - first), prog, logE
             out.append(t)
         return out
 
@@ -305,6 +327,10 @@ class BatchedCircuits:
             if t["kind"] == 0:
                 if (int(t["first"]) + int(t["count"])) << int(t["logRow"]) > size:
                     raise CvdvError("row task outside its instance")
+                if int(t["logE"]) not in loge_options(int(t["logRow"]), self.prec):
+                    raise CvdvError("row task shape the stage kernel does not take")
+                if int(t["count"]) > THREADS // ((1 << int(t["logRow"])) >> int(t["logE"])):
+                    raise CvdvError("row task larger than a CTA")
                 if not (0 <= t["program"] < self.n_programs):
                     raise CvdvError("row task program index out of range")
             else:
@@ -346,29 +372,54 @@ class BatchedCircuits:
             return  # the capture itself does not run: the warm-up call above was the run
         self._graph.replay()
 
+    def _time(self, reps: int) -> float:
+        self._launch_all()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            self._launch_all()
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
     def autotune(self, grids: Sequence[int] = (148, 296), chunks: Sequence[int] = (2048, 8192),
-                 reps: int = 3) -> Tuple[int, int]:
-        """Time every (grid, pair chunk) pair on the compiled batch; keep the fastest.
-        The states are saved and restored around the timing runs."""
+                 reps: int = 3, tune_rows: bool = True) -> Tuple[int, int]:
+        """Time every (grid, pair chunk) pair on the compiled batch and keep the
+        fastest; then, per mode length (largest total work first), every row-task
+        shape loge_options(m) with the others fixed (coordinate descent), keeping
+        the fastest in row_loge.  The states are saved and restored around the
+        timing runs.  Returns (grid, pair chunk); self.tuning records every trial."""
         saved = self.states.clone()
+        self.tuning = {"grid_chunk": [], "row_loge": []}
         best = None
         for chunk in chunks:
             self.pair_chunk = chunk
             self._compile()
             for grid in grids:
                 self.grid = grid
-                self._launch_all()
-                torch.cuda.synchronize()
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record()
-                for _ in range(reps):
-                    self._launch_all()
-                e1.record()
-                e1.synchronize()
-                ms = e0.elapsed_time(e1) / reps
+                ms = self._time(reps)
+                self.tuning["grid_chunk"].append((grid, chunk, ms))
                 if best is None or ms < best[0]:
                     best = (ms, grid, chunk)
-        _, self.grid, self.pair_chunk = best
+        best_ms, self.grid, self.pair_chunk = best
+        if tune_rows:
+            work: Dict[int, int] = {}
+            for inst in self.instances:
+                m = inst["qubits"][-1]
+                work[m] = work.get(m, 0) + (1 << sum(inst["qubits"]))
+            for m in sorted(work, key=lambda k: -work[k]):
+                keep = self.row_loge.get(m, default_loge(m, self.prec))
+                for e in loge_options(m, self.prec):
+                    if e == keep:
+                        continue
+                    self.row_loge[m] = e
+                    self._compile()
+                    ms = self._time(reps)
+                    self.tuning["row_loge"].append((m, e, ms))
+                    if ms < best_ms:
+                        best_ms, keep = ms, e
+                self.row_loge[m] = keep
         self._compile()
         self._graph = None
         self.states.copy_(saved)

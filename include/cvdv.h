@@ -253,7 +253,9 @@ typedef struct {
   int count;             /* rows or pairs */
   int bit;               /* gate: flat bit */
   int program;           /* row program: index into the program table */
-  int pad;
+  int logE;              /* row program: log2 amplitudes per thread (3, 4 or 5: radix-8,
+                            16 or 32 stages, 512 * 2^logE / 2^logRow rows per CTA);
+                            0 = 5 for complex64 rows of 2^13 and more points, else 4 */
   double m[8];           /* gate: 2x2 matrix row-major, (re, im) pairs */
 } CvdvBatchTask;
 

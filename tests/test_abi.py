@@ -145,3 +145,15 @@ def test_error_paths_without_device(lib_path):
     # the allocation-free marginal rejects null pointers before touching the device
     assert lib.cvdvMeasureMultipleNoAlloc(None, 0, ints(1), 1, ints(0), 1, out, None) == 1
     assert list(out) == [7.0, 7.0]
+
+
+def test_batch_row_task_shapes():
+    """Row-task shapes the stage kernel takes: a row fits 512 threads, complex128 at
+    most 16 amplitudes a thread; the defaults are among them."""
+    from cvdv_b200.batch import default_loge, loge_options
+    assert loge_options(8, 1) == [3, 4, 5] and loge_options(14, 1) == [5]
+    assert loge_options(13, 1) == [4, 5] and loge_options(13, 0) == [4]
+    assert loge_options(12, 0) == [3, 4]
+    for prec, top in ((1, 14), (0, 13)):
+        for m in range(8, top + 1):
+            assert default_loge(m, prec) in loge_options(m, prec)

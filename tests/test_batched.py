@@ -61,3 +61,30 @@ def test_batched_graph_replay_and_large_modes():
         ref = _oracle(insts[k], psi0[k])
         got = B.state(k).cpu().numpy()
         assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 2e-5, k
+
+
+@pytest.mark.parametrize("precision,tol", [("complex64", 2e-5), ("complex128", 1e-10)])
+def test_every_row_task_shape_matches_oracle(precision, tol):
+    """Each amplitudes-per-thread choice the autotuner may pick (radix-8, 16 and 32
+    stage schedules, rows per CTA) gives the oracle's result, for every mode length."""
+    from cvdv_b200.batch import BatchedCircuits, loge_options, random_instances
+    from cvdv_b200.cudaCvdv import PRECISIONS
+    prec = PRECISIONS[precision]
+    top = 14 if prec == 1 else 13
+    insts = random_instances(seed=21, count=top - 7, gates=8, m_range=(8, 8))
+    for k, inst in enumerate(insts):  # one instance per mode length 2^8 .. 2^top (same registers)
+        inst["qubits"] = inst["qubits"][:-1] + [8 + k]
+    psi0 = [_initial(i) for i in insts]
+    refs = [_oracle(i, p) for i, p in zip(insts, psi0)]
+    for pick in range(3):
+        shapes = {}
+        for inst in insts:
+            m = inst["qubits"][-1]
+            opts = loge_options(m, prec)
+            shapes[m] = opts[pick % len(opts)]
+        B = BatchedCircuits(insts, precision=precision, row_loge=shapes)
+        B.set_initial(psi0)
+        B.run()
+        for k in range(len(insts)):
+            got = B.state(k).cpu().numpy()
+            assert np.linalg.norm(got - refs[k]) / np.linalg.norm(refs[k]) < tol, (shapes, k)
