@@ -372,10 +372,10 @@ def run_gpu(args, world, rank, local):
     acc_repeated["circuits_applied"] = args.warmup + args.steps
     del sim128, sim64
     torch.cuda.empty_cache()
-    acc_once = state_transfer_accuracy(circ)
+    acc_once = None if args.no_accuracy else state_transfer_accuracy(circ)
 
     extras = {} if args.no_extras else {"gaussian_network_c3": gaussian_c3(args), "batched_c4": batched_c4(args),
-                                         "variational_c5": variational_c5(args)}
+                                         "variational_c5": variational_c5(args), "husimi": husimi_readout(args)}
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -563,7 +563,8 @@ def gaussian_c3(args):
         del sim
         torch.cuda.empty_cache()
     out["value"] = out["complex128"]["value"]
-    out["accuracy_complex64"] = gaussian_c3_accuracy(mq)
+    if not getattr(args, "no_accuracy", False):
+        out["accuracy_complex64"] = gaussian_c3_accuracy(mq)
     return out
 
 
@@ -678,6 +679,38 @@ def variational_c5(args):
                                                       "gradients; FD of the complex128 forward"}}
 
 
+def husimi_readout(args):
+    """Husimi Q of the mode of [1, 10] and [1, 12] (N = 1024, 4096; two slices): the
+    overlap route as one fused pass per output row (cvdvGetHusimiQ), kernel time and
+    wall time including the N^2 read-back."""
+    import numpy as np
+    import torch
+    from cvdv_b200 import CudaCvdv, _lib
+    L = _lib.load()
+    out = {"unit": "ms"}
+    for qubits in ([1, 10], [1, 12]):
+        rng = np.random.default_rng(1)
+        n = sum(qubits)
+        psi = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+        sim = CudaCvdv(qubits, check_errors=True)
+        sim.initFromArray(psi / np.linalg.norm(psi))
+        sim.getHusimiQ(1)
+        L.cvdvSetTiming(sim.ctx, 1)
+        _lib.kernel_stats(sim.ctx)
+        reps = max(3, min(args.steps, 5))
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            sim.getHusimiQ(1)
+        wall = (time.perf_counter() - t0) / reps
+        st = _lib.kernel_stats(sim.ctx)
+        L.cvdvSetTiming(sim.ctx, 0)
+        out[f"N={1 << qubits[1]}"] = {"kernel_ms": (st["phase_space"][0] + st["fft_pass"][0]) / reps,
+                                      "wall_ms": wall * 1e3, "launches": (st["phase_space"][1] + st["fft_pass"][1]) / reps}
+        del sim
+        torch.cuda.empty_cache()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -685,12 +718,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the one-circuit and 200-layer accuracy legs (profiler runs)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched-circuits and variational-gradient measurements")
     ap.add_argument("--workload", default="full", choices=["full", "small"],
                     help="small: 10 qubit registers + the 2^14 mode (2^24 amplitudes), and the two-mode "
                          "network at [12, 12], for ncu")
-    ap.add_argument("--extra", default=None, choices=["c3", "c4", "c5"],
+    ap.add_argument("--extra", default=None, choices=["c3", "c4", "c5", "husimi"],
                     help="run only that extra measurement (one GPU) and print its JSON, for profiling")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -698,7 +733,7 @@ def main():
     world, rank, local = dist_init()
     try:
         if args.extra:
-            fn = {"c3": gaussian_c3, "c4": batched_c4, "c5": variational_c5}[args.extra]
+            fn = {"c3": gaussian_c3, "c4": batched_c4, "c5": variational_c5, "husimi": husimi_readout}[args.extra]
             print(json.dumps({"extra": args.extra, **fn(args)}), flush=True)
         elif args.impl == "reference":
             run_reference(args, world, rank)
