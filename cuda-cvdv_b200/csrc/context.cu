@@ -393,7 +393,7 @@ static bool reads_reg_bits(Context* ctx, const Op& b, int r) {
   return false;
 }
 
-// Pair a row program that ends with a forward 2^14-point transform (four-CTA
+// Pair a row program that ends with a forward 2^14-point transform (cluster
 // kernel) with the next row program on the same register that starts with the
 // inverse one, when everything in between only reads that register through
 // factor tables (qubit gates on other registers, transforms of other registers,
@@ -625,7 +625,7 @@ static bool run_factors(Context* ctx, std::vector<Stage>& stages, std::vector<co
   return true;
 }
 
-// Whether the flush's first op on register r is a four-CTA row program that starts
+// Whether the flush's first op on register r is a cluster row program that starts
 // (after diagonal runs) with an inverse transform, with everything before it
 // reading r only through factor tables; it is then marked to load r blocked.
 static bool starts_blocked(Context* ctx, std::vector<Op>& ops, int r) {

@@ -368,7 +368,7 @@ bool launch_col_chain(Context* ctx, int reg, const std::vector<HostRowOp>& ops);
 // inverse transform; blockedOut: leave it blocked after the final forward transform
 bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops, bool blockedIn = false,
                         bool blockedOut = false);
-// whether launch_row_program runs this program on the four-CTA kernel (which can
+// whether launch_row_program runs this program on the cluster kernel (which can
 // store and load the blocked layout)
 bool rowc_takes(Context* ctx, int reg, const std::vector<HostRowOp>& ops);
 int rowc_log_cluster();  // log2 CTAs per 2^14-point complex128 row (the blocked layout's permLogC)

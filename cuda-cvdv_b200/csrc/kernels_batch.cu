@@ -69,6 +69,16 @@ __device__ __forceinline__ double2 ft_twiddle(int j, int N, int sign) {
   return make_double2(c, s);
 }
 
+// Ratio of ft_twiddle between j + d and j: exp(i sign pi (N-1) d / N), the angle
+// reduced exactly in integers.  A thread's points t + k TPR take the twiddle as a
+// running product from its exact value at t (16 steps: a few units of 1e-16).
+__device__ __forceinline__ double2 ft_twiddle_step(int d, int N, int sign) {
+  const long long m = ((long long)(N - 1) * d) % (2LL * N);
+  double s, c;
+  sincospi((double)sign * (double)m / (double)N, &s, &c);
+  return make_double2(c, s);
+}
+
 // ---------------------------------------------------------------- Rx
 template <typename C>
 __global__ void __launch_bounds__(kBatchThreads) k_b_rx(C* __restrict__ st, uint64_t nPairs, int n, int bit,
@@ -148,6 +158,14 @@ __device__ __forceinline__ double2 b_kick(int k, int N, double coef) {
   return make_double2(c * inv, s * inv);
 }
 
+// exp(i coef dx d): the ratio of b_kick between k + d and k
+__device__ __forceinline__ double2 b_kick_step(int d, int N, double coef) {
+  const double dx = sqrt(2.0 * M_PI / (double)N);
+  double s, c;
+  sincos(coef * dx * (double)d, &s, &c);
+  return make_double2(c, s);
+}
+
 template <typename C, int LOGQ>
 __global__ void __launch_bounds__(BRow<LOGQ>::NT, 2)
     k_b_cd(C* __restrict__ st, uint64_t nRows, int n, int ctrlBit, const double* __restrict__ beta, double sign) {
@@ -168,20 +186,30 @@ __global__ void __launch_bounds__(BRow<LOGQ>::NT, 2)
   b_fill_twiddles<LOGQ>(lo, tid, G::NT);
   C v[16];
 #pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = st[rowBase + t + k * TPR];
+  const double2 tw0 = ft_twiddle(t, N, 1), tws = ft_twiddle_step(TPR, N, 1);
+  double2 f = tw0;
+#pragma unroll
   for (int k = 0; k < 16; ++k) {
-    const int j = t + k * TPR;
-    v[k] = cmul(st[rowBase + j], fromd<C>(ft_twiddle(j, N, 1)));
+    v[k] = cmul(v[k], fromd<C>(f));
+    f = dmul(f, tws);
   }
   __syncthreads();
   rr_stages<C, 1, LOGQ, 0, 4>(v, smrow, t, lo, hi);
-#pragma unroll
-  for (int k = 0; k < 16; ++k) v[k] = cmul(v[k], fromd<C>(b_kick(t + k * TPR, N, coef)));
-  rr_stages<C, -1, LOGQ, 0, 4>(v, smrow, t, lo, hi);
-  if (!valid) return;
+  f = b_kick(t, N, coef);
+  const double2 ks = b_kick_step(TPR, N, coef);
 #pragma unroll
   for (int k = 0; k < 16; ++k) {
-    const int j = t + k * TPR;
-    st[rowBase + j] = cmul(v[k], fromd<C>(ft_twiddle(j, N, -1)));
+    v[k] = cmul(v[k], fromd<C>(f));
+    f = dmul(f, ks);
+  }
+  rr_stages<C, -1, LOGQ, 0, 4>(v, smrow, t, lo, hi);
+  if (!valid) return;
+  f = cconj(tw0);  // ft_twiddle(j, N, -1) = conj(ft_twiddle(j, N, 1))
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    st[rowBase + t + k * TPR] = cmul(v[k], fromd<C>(f));
+    f = dmul(f, cconj(tws));
   }
 }
 
@@ -210,24 +238,33 @@ __global__ void __launch_bounds__(BRow<LOGQ>::NT, 1)
   const double coef = -__ldg(beta + b) * kz;      // exp(-i beta K)
   const double dx = sqrt(2.0 * M_PI / (double)N);
   b_fill_twiddles<LOGQ>(lo, tid, G::NT);
+  const double2 tw0 = ft_twiddle(t, N, 1), tws = ft_twiddle_step(TPR, N, 1);
   C v[16];
 #pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = psi[rowBase + t + k * TPR];
+  double2 f = tw0;
+#pragma unroll
   for (int k = 0; k < 16; ++k) {
-    const int j = t + k * TPR;
-    v[k] = cmul(psi[rowBase + j], fromd<C>(ft_twiddle(j, N, 1)));
+    v[k] = cmul(v[k], fromd<C>(f));
+    f = dmul(f, tws);
   }
   __syncthreads();
   rr_stages<C, 1, LOGQ, 0, 4>(v, smrow, t, lo, hi);
 #pragma unroll
   for (int k = 0; k < 16; ++k) krow[t + k * TPR] = v[k];
 #pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = lam[rowBase + t + k * TPR];
+  f = tw0;
+#pragma unroll
   for (int k = 0; k < 16; ++k) {
-    const int j = t + k * TPR;
-    v[k] = cmul(lam[rowBase + j], fromd<C>(ft_twiddle(j, N, 1)));
+    v[k] = cmul(v[k], fromd<C>(f));
+    f = dmul(f, tws);
   }
   rr_stages<C, 1, LOGQ, 0, 4>(v, smrow, t, lo, hi);
   // <F lambda| K |F psi> = (1/N) sum_k conj(L_k) K_k P_k for the unnormalised transforms
   double gx = 0.0, gy = 0.0;
+  f = b_kick(t, N, coef);
+  const double2 ks = b_kick_step(TPR, N, coef);
 #pragma unroll
   for (int k = 0; k < 16; ++k) {
     const int kk = t + k * TPR;
@@ -235,26 +272,29 @@ __global__ void __launch_bounds__(BRow<LOGQ>::NT, 1)
     const double w = kz * ((double)kk - 0.5 * (double)(N - 1)) * dx / (double)N;
     gx += w * (L.x * P.x + L.y * P.y);
     gy += w * (L.x * P.y - L.y * P.x);
-    const C f = fromd<C>(b_kick(kk, N, coef));
-    v[k] = cmul(v[k], f);
-    krow[kk] = cmul(krow[kk], f);
+    const C fc = fromd<C>(f);
+    v[k] = cmul(v[k], fc);
+    krow[kk] = cmul(krow[kk], fc);
+    f = dmul(f, ks);
   }
   rr_stages<C, -1, LOGQ, 0, 4>(v, smrow, t, lo, hi);
   if (valid) {
+    f = cconj(tw0);  // ft_twiddle(j, N, -1) = conj(ft_twiddle(j, N, 1))
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
-      const int j = t + k * TPR;
-      lam[rowBase + j] = cmul(v[k], fromd<C>(ft_twiddle(j, N, -1)));
+      lam[rowBase + t + k * TPR] = cmul(v[k], fromd<C>(f));
+      f = dmul(f, cconj(tws));
     }
   }
 #pragma unroll
   for (int k = 0; k < 16; ++k) v[k] = krow[t + k * TPR];
   rr_stages<C, -1, LOGQ, 0, 4>(v, smrow, t, lo, hi);
   if (valid) {
+    f = cconj(tw0);
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
-      const int j = t + k * TPR;
-      psi[rowBase + j] = cmul(v[k], fromd<C>(ft_twiddle(j, N, -1)));
+      psi[rowBase + t + k * TPR] = cmul(v[k], fromd<C>(f));
+      f = dmul(f, cconj(tws));
     }
   }
   // per-row sum: lanes of one row (TPR >= 16 consecutive threads), then the row's warps

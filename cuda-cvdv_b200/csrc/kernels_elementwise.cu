@@ -299,18 +299,32 @@ __device__ __forceinline__ uint64_t perm_src(const PermDesc& P, uint64_t i) {
   return (i & ~(m1 | m2)) | (b << P.shift1) | (a << P.shift2);
 }
 
+// Each thread issues its V gathers before evaluating any factor, so V loads are in
+// flight per thread.
 template <typename C>
 __global__ void __launch_bounds__(256) k_perm(const C* __restrict__ in, C* __restrict__ out,
                                              uint64_t n, PermDesc P, FactorList pre,
                                              FactorList post) {
+  constexpr int V = 4;
   const bool hasPre = !factor_empty(pre), hasPost = !factor_empty(post);
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (uint64_t)gridDim.x * blockDim.x) {
-    uint64_t s = perm_src(P, i);
-    C v = in[s];
-    if (hasPre) v = cmul(v, fromd<C>(eval_factor(pre, s)));
-    if (hasPost) v = cmul(v, fromd<C>(eval_factor(post, i)));
-    out[i] = v;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x * V;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x * V + threadIdx.x; base < n; base += stride) {
+    C v[V];
+    uint64_t s[V];
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+      const uint64_t i = base + (uint64_t)k * blockDim.x;
+      s[k] = i < n ? perm_src(P, i) : 0;
+      if (i < n) v[k] = in[s[k]];
+    }
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+      const uint64_t i = base + (uint64_t)k * blockDim.x;
+      if (i >= n) continue;
+      if (hasPre) v[k] = cmul(v[k], fromd<C>(eval_factor(pre, s[k])));
+      if (hasPost) v[k] = cmul(v[k], fromd<C>(eval_factor(post, i)));
+      out[i] = v[k];
+    }
   }
 }
 

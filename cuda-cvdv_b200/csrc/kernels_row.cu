@@ -88,7 +88,7 @@ struct RowProgram {
   int nDiag;
   int logTwN;
   int loadT;    // cluster rows: start transposed (1: from the natural layout, 2: from the blocked one)
-  int storeBlocked;  // four-CTA rows ending transposed: write the blocked layout
+  int storeBlocked;  // cluster rows ending transposed: write the blocked layout
   int logS;          // k_rowr on a strided register: log2 of the amplitudes below it (0: rows)
   const double2* tw;
   unsigned int* waitErr;  // set when a bounded wait on the cluster peers gives up
@@ -656,38 +656,38 @@ bool col_program_ok(Context* ctx, int reg) {
   return ctx->totalQbt - q >= logR;
 }
 
-// ---------------------------------------------------------------- four-CTA register-resident rows
-// A row of N = 4 M points is split over a cluster of four CTAs of M / 16 threads
-// (2^14-point complex128 rows: 4096 points and 256 threads per CTA, 72 KB of
-// shared memory, so CTAs of two clusters share an SM and one row's loads and
-// stores run while the other row's butterflies do).  Every thread keeps 16
-// amplitudes in registers.  With Q = M / 4 and m_i = r Q + t + TPR i for thread t
-// of CTA r (i < 4), two layouts occur:
-//   S ("strips"):     v[4 j1 + i] = x[j1 M + m_i]   (CTA r holds quarter r of
-//                     each quarter-row: coalesced loads and stores)
-//   T ("transposed"): v[w] = X[r + 4 k2] at k2 = t + TPR w   (w < 16)
-// Forward, S -> T: radix-4 butterflies over j1 in registers give
-//   y_k1[m_i] = w_N^{m_i k1} sum_j1 w_4^{j1 k1} x[j1 M + m_i];
+// ---------------------------------------------------------------- cluster register-resident rows
+// A row of N = C M points is split over a cluster of C CTAs of M / 16 threads
+// (2^14-point complex128 rows: C = 8, 2048 points and 128 threads per CTA, 38 KB
+// of shared memory, so CTAs of four clusters share an SM and the rows' loads,
+// exchanges and butterflies overlap).  Every thread keeps 16 amplitudes in
+// registers.  With I = 16 / C, Q = M / C and m_i = r Q + t + TPR i for thread t
+// of CTA r (i < I), two layouts occur:
+//   S ("strips"):     v[I j1 + i] = x[j1 M + m_i]   (CTA r holds part r of each
+//                     C-th of the row: coalesced loads and stores)
+//   T ("transposed"): v[w] = X[r + C k2] at k2 = t + TPR w   (w < 16)
+// Forward, S -> T: radix-C butterflies over j1 in registers give
+//   y_k1[m_i] = w_N^{m_i k1} sum_j1 w_C^{j1 k1} x[j1 M + m_i];
 //   thread t hands y_k1[m_i] (k1 != r) to thread t of CTA k1, after which every
 //   thread holds y_r[t + TPR k] for all 16 k, and an M-point DFT of y_r gives
-//   X[r + 4 k2] in the natural Stockham order.
+//   X[r + C k2] in the natural Stockham order.
 // Inverse, T -> S: an M-point inverse DFT gives z_r[m] at m = t + TPR w; thread t
-//   hands z_r[m] for CTA q's quarter (w = 4 q + i) to thread t of CTA q, then
-//   x[j1 M + m_i] = sum_k1 w_4^{-j1 k1} w_N^{-m_i k1} z_k1[m_i]   (radix-4 again).
-// So each transform moves 12 of a thread's 16 amplitudes once, and only between
-// threads of the same index: the sender writes them straight into the receiving
-// CTA's shared memory (slot (4 src + i) TPR + t) between two cluster barriers; the
-// 4 it keeps never leave its registers.  Diagonal runs in T read tables stored
-// permuted for four CTAs (position r M + k2 holds index r + 4 k2).
-template <typename C, int LOGM>
+//   hands z_r[m] for CTA q's part (w = I q + i) to thread t of CTA q, then
+//   x[j1 M + m_i] = sum_k1 w_C^{-j1 k1} w_N^{-m_i k1} z_k1[m_i]   (radix C again).
+// So each transform moves 16 - I of a thread's 16 amplitudes once, and only
+// between threads of the same index: the sender writes them straight into the
+// receiving CTA's shared memory (slot (I src + i) TPR + t); the I it keeps never
+// leave its registers.  Diagonal runs in T read tables stored permuted for C CTAs
+// (position r M + k2 holds index r + C k2).
+template <typename C, int LOGM, int LOGC>
 __device__ __forceinline__ void rq_diag(C (&v)[16], const RowDiag& D, uint64_t rowBase, int t, int r,
                                         bool layoutT) {
-  constexpr int M = 1 << LOGM, TPR = M / 16, Q = M / 4;
+  constexpr int M = 1 << LOGM, TPR = M / 16, IPS = 16 >> LOGC, Q = M >> LOGC;
   const double2 rs = D.hasRowF ? eval_factor(D.rowF, rowBase) : make_double2(1.0, 0.0);
   if (D.tab) {
     int seg = 0;
     for (int c = 0; c < D.nCtrl; ++c) seg |= (int)((rowBase >> D.ctrlShift[c]) & 1ull) << c;
-    const double2* tp = D.tab + ((size_t)seg << (LOGM + 2));
+    const double2* tp = D.tab + ((size_t)seg << (LOGM + LOGC));
     // T: permuted table at r M + k2; S: natural index j1 M + r Q + t + TPR i
     const double2* base = layoutT ? tp + r * M + t : tp + r * Q + t;
 #pragma unroll
@@ -696,7 +696,7 @@ __device__ __forceinline__ void rq_diag(C (&v)[16], const RowDiag& D, uint64_t r
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
         const int kk = k0 + k;
-        w[k] = __ldg(base + (layoutT ? TPR * kk : (kk >> 2) * M + TPR * (kk & 3)));
+        w[k] = __ldg(base + (layoutT ? TPR * kk : (kk / IPS) * M + TPR * (kk % IPS)));
       }
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
@@ -762,40 +762,61 @@ __device__ __forceinline__ void mbar_wait_bounded(uint32_t bar, uint32_t parity,
   if (err) atomicOr(err, 1u);
 }
 
-// Thread t hands its 12 amplitudes v[4 q + i] (q != r) to thread t of CTA q, slot
-// (4 r + i) TPR + t of that CTA's buffer, and takes v[4 q + i] from slot
-// (4 q + i) TPR + t of its own, which thread t of CTA q wrote.  The writes are
-// st.async into the peer's shared memory, each completing 16 (complex128) or 8
-// bytes on the peer's mbarrier, which expects 12 TPR amplitudes per exchange; so a
-// CTA waits only for its own data, with no cluster-wide barrier or fence.  The
-// caller has arrived on the cluster barrier once its buffer was free (at start,
-// or after its last local use); the wait here orders the remote writes after
-// every peer's arrival.
-template <typename C, int TPR>
+// Thread t hands its amplitudes v[I q + i] (q != r, i < I = 16 / C) to thread t of
+// CTA q, slot (I r + i) TPR + t of that CTA's buffer, and takes v[I q + i] from
+// slot (I q + i) TPR + t of its own, which thread t of CTA q wrote.  The writes
+// are st.async into the peer's shared memory, each completing 16 (complex128) or
+// 8 bytes on the peer's mbarrier, which expects (16 - I) TPR amplitudes per
+// exchange; so a CTA waits only for its own data, with no cluster-wide barrier or
+// fence.  The caller has arrived on the cluster barrier once its buffer was free
+// (at start, or after its last local use); the wait here orders the remote writes
+// after every peer's arrival.
+template <typename C, int TPR, int LOGC>
 __device__ __forceinline__ void rq_exchange(C (&v)[16], C* buf, uint32_t bar, uint32_t& parity, int t, int r,
                                             unsigned int* err) {
-  if (t == 0) mbar_expect_tx(bar, 12u * TPR * (uint32_t)sizeof(C));
+  constexpr int NC = 1 << LOGC, IPS = 16 >> LOGC;
+  if (t == 0) mbar_expect_tx(bar, (uint32_t)((16 - IPS) * TPR * sizeof(C)));
   cluster_wait_acquire();
   const uint32_t base = smem_addr(buf), rbar = bar;
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
+  for (int q = 0; q < NC; ++q) {
     if (q == r) continue;
     const uint32_t dst = cluster_map(base, q), dbar = cluster_map(rbar, q);
 #pragma unroll
-    for (int i = 0; i < 4; ++i) st_async(dst + (uint32_t)(((4 * r + i) * TPR + t) * sizeof(C)), v[4 * q + i], dbar);
+    for (int i = 0; i < IPS; ++i)
+      st_async(dst + (uint32_t)(((IPS * r + i) * TPR + t) * sizeof(C)), v[IPS * q + i], dbar);
   }
   mbar_wait_bounded(bar, parity, err);
   parity ^= 1u;
 #pragma unroll
   for (int k = 0; k < 16; ++k)
-    if ((k >> 2) != r) v[k] = buf[k * TPR + t];
+    if (k / IPS != r) v[k] = buf[k * TPR + t];
   __syncthreads();  // every thread has read its slots before the buffer is reused
 }
 
-template <typename C, int LOGN>
-__global__ void __launch_bounds__(1 << (LOGN - 6), 2)
+// radix-C butterfly across the cluster at point i of every strip: forward
+// y_k1 = w_N^{m k1} sum_j1 w_C^{j1 k1} x_j1, inverse x_j1 = sum_k1 w_C^{-j1 k1} w_N^{-m k1} z_k1
+template <typename C, int DIR, int LOGC>
+__device__ __forceinline__ void rq_cross(C (&v)[16], int i, const double2* loN, const double2* hiN, int m) {
+  constexpr int NC = 1 << LOGC, IPS = 16 >> LOGC;
+  C a[NC], w[NC];
+  w[0] = mk((decltype(v[0].x))1, (decltype(v[0].x))0);
+  w[1] = tw2<C, DIR>(loN, hiN, m);
+#pragma unroll
+  for (int k = 2; k < NC; ++k) w[k] = cmul(w[k >> 1], w[k - (k >> 1)]);
+#pragma unroll
+  for (int j = 0; j < NC; ++j) a[j] = DIR > 0 ? v[IPS * j + i] : cmul(v[IPS * j + i], w[j]);
+  if constexpr (NC == 4) bf4<C, DIR>(a[0], a[1], a[2], a[3]);
+  else if constexpr (NC == 8) bf8<C, DIR>(a);
+  else bf16<C, DIR>(a);
+#pragma unroll
+  for (int j = 0; j < NC; ++j) v[IPS * j + i] = DIR > 0 ? cmul(a[j], w[j]) : a[j];
+}
+
+template <typename C, int LOGN, int LOGC>
+__global__ void __launch_bounds__(1 << (LOGN - LOGC - 4), 1 << (LOGC - 1))
     k_rowq(const C* __restrict__ in, C* __restrict__ out, uint64_t nRows, const __grid_constant__ RowProgram P) {
-  constexpr int LOGM = LOGN - 2, M = 1 << LOGM, TPR = M / 16, Q = M / 4;
+  constexpr int LOGM = LOGN - LOGC, M = 1 << LOGM, TPR = M / 16, NC = 1 << LOGC, IPS = 16 >> LOGC, Q = M >> LOGC;
   constexpr int RS = M + (M >> 4);
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
@@ -803,7 +824,7 @@ __global__ void __launch_bounds__(1 << (LOGN - 6), 2)
   double2* hiM = loM + 64;                              // w_M^(64 h), h < M / 64
   double2* loN = hiM + (M >> 6);                        // w_N^e, e < 64
   double2* hiN = loN + 64;                              // w_N^(64 h), h < M / 64
-  __shared__ __align__(8) uint64_t xbar;  // completes when the peers' 12 TPR amplitudes have landed
+  __shared__ __align__(8) uint64_t xbar;  // completes when the peers' (16 - I) TPR amplitudes have landed
   cg::cluster_group cl = cg::this_cluster();
   const int r = (int)cl.block_rank();
   const int t = threadIdx.x;
@@ -833,61 +854,43 @@ __global__ void __launch_bounds__(1 << (LOGN - 6), 2)
       break;
     }
   // persistent clusters: cluster c takes rows c, c + nClusters, ...
-  const uint64_t nClusters = gridDim.x >> 2;
-  for (uint64_t row = blockIdx.x >> 2; row < nRows; row += nClusters) {
+  const uint64_t nClusters = gridDim.x >> LOGC;
+  for (uint64_t row = blockIdx.x >> LOGC; row < nRows; row += nClusters) {
     const uint64_t rowBase = row << LOGN;
     bool arrived = fwdFirst;
     if (arrived) cluster_arrive_release();
     C v[16];
     bool layoutT = P.loadT != 0;
-    if (P.loadT == 2) {  // blocked: X[r + 4 k2] contiguous at r M + k2
+    if (P.loadT == 2) {  // blocked: X[r + C k2] contiguous at r M + k2
 #pragma unroll
       for (int w = 0; w < 16; ++w) v[w] = in[rowBase + (uint64_t)r * M + t + TPR * w];
-    } else if (P.loadT == 1) {  // transposed from the natural layout (every fourth element)
+    } else if (P.loadT == 1) {  // transposed from the natural layout (every C-th element)
 #pragma unroll
-      for (int w = 0; w < 16; ++w) v[w] = in[rowBase + r + 4 * (uint64_t)(t + TPR * w)];
+      for (int w = 0; w < 16; ++w) v[w] = in[rowBase + r + NC * (uint64_t)(t + TPR * w)];
     } else {
 #pragma unroll
-      for (int k = 0; k < 16; ++k) v[k] = in[rowBase + (uint64_t)(k >> 2) * M + r * Q + t + TPR * (k & 3)];
+      for (int k = 0; k < 16; ++k) v[k] = in[rowBase + (uint64_t)(k / IPS) * M + r * Q + t + TPR * (k % IPS)];
     }
 
     for (int o = 0; o < P.nOps; ++o) {
       const RowOp& op = P.ops[o];
       if (op.kind == kRowDiag) {
-        rq_diag<C, LOGM>(v, P.diag[op.diag], rowBase, t, r, layoutT);
+        rq_diag<C, LOGM, LOGC>(v, P.diag[op.diag], rowBase, t, r, layoutT);
       } else if (op.dir > 0) {  // S -> T
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          C a0 = v[i], a1 = v[4 + i], a2 = v[8 + i], a3 = v[12 + i];
-          bf4<C, 1>(a0, a1, a2, a3);
-          const C w1 = tw2<C, 1>(loN, hiN, r * Q + t + TPR * i);
-          const C w2 = cmul(w1, w1);
-          v[i] = a0;
-          v[4 + i] = cmul(a1, w1);
-          v[8 + i] = cmul(a2, w2);
-          v[12 + i] = cmul(a3, cmul(w2, w1));
-        }
+        for (int i = 0; i < IPS; ++i) rq_cross<C, 1, LOGC>(v, i, loN, hiN, r * Q + t + TPR * i);
         if (!arrived) cluster_arrive_release();  // this CTA is done with its buffer
-        rq_exchange<C, TPR>(v, sm, bar, parity, t, r, P.waitErr);
+        rq_exchange<C, TPR, LOGC>(v, sm, bar, parity, t, r, P.waitErr);
         arrived = false;
         rr_stages<C, 1, LOGM, 0, 4>(v, sm, t, loM, hiM);
         layoutT = true;
       } else {  // T -> S
         rr_stages<C, -1, LOGM, 0, 4>(v, sm, t, loM, hiM);
         if (!arrived) cluster_arrive_release();
-        rq_exchange<C, TPR>(v, sm, bar, parity, t, r, P.waitErr);
+        rq_exchange<C, TPR, LOGC>(v, sm, bar, parity, t, r, P.waitErr);
         arrived = false;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const C w1 = tw2<C, -1>(loN, hiN, r * Q + t + TPR * i);
-          const C w2 = cmul(w1, w1);
-          C a0 = v[i], a1 = cmul(v[4 + i], w1), a2 = cmul(v[8 + i], w2), a3 = cmul(v[12 + i], cmul(w2, w1));
-          bf4<C, -1>(a0, a1, a2, a3);
-          v[i] = a0;
-          v[4 + i] = a1;
-          v[8 + i] = a2;
-          v[12 + i] = a3;
-        }
+        for (int i = 0; i < IPS; ++i) rq_cross<C, -1, LOGC>(v, i, loN, hiN, r * Q + t + TPR * i);
         layoutT = false;
       }
     }
@@ -895,24 +898,25 @@ __global__ void __launch_bounds__(1 << (LOGN - 6), 2)
     if (arrived) cluster_wait_acquire();  // pair an arrival no exchange waited for
     if (!layoutT) {
 #pragma unroll
-      for (int k = 0; k < 16; ++k) out[rowBase + (uint64_t)(k >> 2) * M + r * Q + t + TPR * (k & 3)] = v[k];
+      for (int k = 0; k < 16; ++k) out[rowBase + (uint64_t)(k / IPS) * M + r * Q + t + TPR * (k % IPS)] = v[k];
     } else if (P.storeBlocked) {
 #pragma unroll
       for (int w = 0; w < 16; ++w) out[rowBase + (uint64_t)r * M + t + TPR * w] = v[w];
     } else {
 #pragma unroll
-      for (int w = 0; w < 16; ++w) out[rowBase + r + 4 * (uint64_t)(t + TPR * w)] = v[w];
+      for (int w = 0; w < 16; ++w) out[rowBase + r + NC * (uint64_t)(t + TPR * w)] = v[w];
     }
     // The next row's first arrival says this CTA's buffer is free again: the last
     // reads of it (the last exchange or stage) ended in a CTA barrier.
   }
 }
-template <typename C, int LOGN>
+template <typename C, int LOGN, int LOGC>
 static cudaError_t launch_rowq_t(Context* ctx, const RowProgram& P) {
-  constexpr int M = 1 << (LOGN - 2);
+  constexpr int M = 1 << (LOGN - LOGC), NC = 1 << LOGC;
   const size_t smem = (size_t)(M + (M >> 4)) * sizeof(C) + 2 * (64 + (M >> 6)) * sizeof(double2);
-  auto kern = k_rowq<C, LOGN>;
+  auto kern = k_rowq<C, LOGN, LOGC>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess && NC > 8) e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   if (e != cudaSuccess) return e;
   const uint64_t nRows = ctx->size() >> LOGN;
   cudaLaunchConfig_t cfg{};
@@ -921,7 +925,7 @@ static cudaError_t launch_rowq_t(Context* ctx, const RowProgram& P) {
   cfg.stream = ctx->stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = 4;
+  attr[0].val.clusterDim.x = NC;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
@@ -931,14 +935,14 @@ static cudaError_t launch_rowq_t(Context* ctx, const RowProgram& P) {
   static int clusters[64] = {};
   const int dev = ctx->device >= 0 && ctx->device < 64 ? ctx->device : 0;
   if (!clusters[dev]) {
-    cfg.gridDim = dim3((unsigned)(4 * 1024));
+    cfg.gridDim = dim3((unsigned)(NC * 1024));
     int n = 0;
     e = cudaOccupancyMaxActiveClusters(&n, kern, &cfg);
     if (e != cudaSuccess) return e;
     clusters[dev] = n > 0 ? n : 1;
   }
   const uint64_t nc = nRows < (uint64_t)clusters[dev] ? nRows : (uint64_t)clusters[dev];
-  cfg.gridDim = dim3((unsigned)(4 * nc));
+  cfg.gridDim = dim3((unsigned)(NC * nc));
   return cudaLaunchKernelEx(&cfg, kern, (const C*)ctx->state(), (C*)ctx->other(), nRows, P);
 }
 
@@ -1059,7 +1063,7 @@ static cudaError_t launch_row_t(Context* ctx, const RowProgram& P, uint64_t nCta
   return cudaLaunchKernelEx(&cfg, kern, (const C*)ctx->state(), (C*)ctx->other(), P);
 }
 
-// 2^14-point complex128 rows run on the four-CTA kernel (k_rowq).  Complex64 rows
+// 2^14-point complex128 rows run on the eight-CTA kernel (k_rowq).  Complex64 rows
 // of that length fit one CTA, k_rowr, which measured faster for them than k_rowq
 // (2.0 against 1.5 ms per 2^28-amplitude launch).
 static bool rowc_shape(Context* ctx, int reg, const std::vector<HostRowOp>& ops) {
@@ -1073,9 +1077,9 @@ static bool rowc_shape(Context* ctx, int reg, const std::vector<HostRowOp>& ops)
   return true;
 }
 
-// log2 of the cluster that runs 2^14-point complex128 row programs (k_rowq: four
-// 256-thread CTAs); the blocked layout between paired programs follows it.
-int rowc_log_cluster() { return 2; }
+// log2 of the cluster that runs 2^14-point complex128 row programs (k_rowq: eight
+// 128-thread CTAs); the blocked layout between paired programs follows it.
+int rowc_log_cluster() { return 3; }
 
 bool rowc_takes(Context* ctx, int reg, const std::vector<HostRowOp>& ops) {
   if (!rowc_shape(ctx, reg, ops)) return false;
@@ -1208,10 +1212,10 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
   bool elemF = false;
   for (int d = 0; d < P.nDiag; ++d) elemF |= P.diag[d].hasElemF != 0;
   if ((blockedIn || blockedOut) && !useC) {
-    set_error(ctx, kErrUnsupported, "blocked layout requested for a program the four-CTA kernel does not run");
+    set_error(ctx, kErrUnsupported, "blocked layout requested for a program the cluster kernel does not run");
     return false;
   }
-  // the four-CTA kernel needs transforms that alternate in direction (each forward
+  // the cluster kernel needs transforms that alternate in direction (each forward
   // leaves the transposed layout an inverse consumes)
   bool alternating = true;
   int lastDir = 0;
@@ -1226,7 +1230,7 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
     cudaError_t er;
     {
       LaunchScope _ls(ctx, kKFft);
-      er = launch_rowq_t<double2, 14>(ctx, P);
+      er = launch_rowq_t<double2, 14, 3>(ctx, P);
     }
     if (!cuda_ok(ctx, er, "row program launch")) return false;
     ctx->cur ^= 1;

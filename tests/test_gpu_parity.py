@@ -289,7 +289,8 @@ COLUMN_GATES = [("d", (1, 0.3 + 0.2j)), ("r", (1, 0.7)), ("s", (2, 0.3)), ("bs",
                 ("phaseCubic", (1, 0.01)), ("r", (1, -1.4)), ("cd", (2, 0, 0, -0.3 + 0.2j))]
 
 
-@pytest.mark.parametrize("qubits", [[1, 9, 8, 3], [1, 13, 8, 0], [1, 8, 13, 0], [1, 10, 9, 4], [1, 14, 3, 0]])
+@pytest.mark.parametrize("qubits", [[1, 9, 8, 3], [1, 13, 8, 0], [1, 8, 13, 0], [1, 10, 9, 4], [1, 14, 3, 0],
+                                    [1, 12, 5, 0], [1, 11, 3, 2], [1, 11, 2, 3]])
 def test_column_programs(qubits):
     """Runs of transforms and diagonal gates on strided registers (beam splitters
     between two of them, controls from a qubit register) as one on-chip pass per
