@@ -78,6 +78,9 @@ struct RowDiag {
   int nLin;
   double regC, regDx;
   XXFactor lin[kMaxXX];
+  // k_rowq: a run whose register terms are only transform twiddles (no table):
+  // the sum of their signs s, the factor exp(i pi s (N-1)(2n-N+1)/(2N)) at point n
+  int ftSign;
 };
 
 struct RowProgram {
@@ -679,11 +682,57 @@ bool col_program_ok(Context* ctx, int reg) {
 // receiving CTA's shared memory (slot (I src + i) TPR + t); the I it keeps never
 // leave its registers.  Diagonal runs in T read tables stored permuted for C CTAs
 // (position r M + k2 holds index r + C k2).
+// exp(i pi s (N-1)(2n-N+1)/(2N)) with the angle reduced exactly in integers, and
+// its ratio between n + d and n, exp(i pi s (N-1) d / N)
+__device__ __forceinline__ double2 ft_tw_at(long long n, long long N, int s) {
+  long long m = ((N - 1) * (2 * n - N + 1) * s) % (4 * N);
+  if (m < 0) m += 4 * N;
+  double sn, c;
+  sincospi((double)m / (double)(2 * N), &sn, &c);
+  return make_double2(c, sn);
+}
+__device__ __forceinline__ double2 ft_tw_ratio(long long d, long long N, int s) {
+  long long m = ((N - 1) * d * s) % (2 * N);
+  if (m < 0) m += 2 * N;
+  double sn, c;
+  sincospi((double)m / (double)N, &sn, &c);
+  return make_double2(c, sn);
+}
+
 template <typename C, int LOGM, int LOGC>
 __device__ __forceinline__ void rq_diag(C (&v)[16], const RowDiag& D, uint64_t rowBase, int t, int r,
                                         bool layoutT) {
-  constexpr int M = 1 << LOGM, TPR = M / 16, IPS = 16 >> LOGC, Q = M >> LOGC;
+  constexpr int M = 1 << LOGM, TPR = M / 16, IPS = 16 >> LOGC, Q = M >> LOGC, NC = 1 << LOGC;
+  constexpr long long N = (long long)M << LOGC;
   const double2 rs = D.hasRowF ? eval_factor(D.rowF, rowBase) : make_double2(1.0, 0.0);
+  if (D.ftSign) {
+    // transform twiddles as running products from exact values (a thread's points
+    // are arithmetic progressions in n): T holds n = r + C (t + TPR w), S holds
+    // n = j1 M + r Q + t + TPR i at v[I j1 + i]
+    if (layoutT) {
+      double2 f = dmul(ft_tw_at(r + NC * t, N, D.ftSign), rs);
+      const double2 st = ft_tw_ratio((long long)NC * TPR, N, D.ftSign);
+#pragma unroll
+      for (int w = 0; w < 16; ++w) {
+        v[w] = cmul(v[w], fromd<C>(f));
+        f = dmul(f, st);
+      }
+    } else {
+      double2 f = dmul(ft_tw_at(r * Q + t, N, D.ftSign), rs);
+      const double2 si = ft_tw_ratio(TPR, N, D.ftSign), sj = ft_tw_ratio(M, N, D.ftSign);
+#pragma unroll
+      for (int j1 = 0; j1 < NC; ++j1) {
+        double2 g = f;
+#pragma unroll
+        for (int i = 0; i < IPS; ++i) {
+          v[IPS * j1 + i] = cmul(v[IPS * j1 + i], fromd<C>(g));
+          g = dmul(g, si);
+        }
+        f = dmul(f, sj);
+      }
+    }
+    return;
+  }
   if (D.tab) {
     int seg = 0;
     for (int c = 0; c < D.nCtrl; ++c) seg |= (int)((rowBase >> D.ctrlShift[c]) & 1ull) << c;
@@ -1168,6 +1217,14 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
     for (int c = 0; c < D.nCtrl; ++c) D.ctrlShift[c] = bits[c];
     D.tab = nullptr;
     D.permuted = opTransposed ? 1 : 0;
+    D.ftSign = 0;
+    // on the cluster kernel a run of transform twiddles alone needs no table
+    bool twOnly = useC && !regTerms.empty() && bits.empty();
+    for (const Term& t : regTerms) twOnly &= t.kind == kTermFtTw;
+    if (twOnly) {
+      for (const Term& t : regTerms) D.ftSign += t.sign;
+      regTerms.clear();
+    }
     if (!regTerms.empty()) {
       double2* tab = (double2*)arena_alloc(ctx, ((size_t)1 << (q + D.nCtrl)) * sizeof(double2));
       if (!tab) return false;
