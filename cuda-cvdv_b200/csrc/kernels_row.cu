@@ -78,9 +78,14 @@ struct RowDiag {
   int nLin;
   double regC, regDx;
   XXFactor lin[kMaxXX];
-  // k_rowq: a run whose register terms are only transform twiddles (no table):
-  // the sum of their signs s, the factor exp(i pi s (N-1)(2n-N+1)/(2N)) at point n
+  // k_rowq: a run whose register terms are linear phases (no table): transform
+  // twiddles, the sum of their signs s giving exp(i pi s (N-1)(2n-N+1)/(2N)) at
+  // point n, and terms c x_n (x_n = (n - regC) regDx), each negated when its
+  // control bit (a row bit, or none: -1) is set
   int ftSign;
+  int nPl;
+  double plC[2];
+  int plCtrl[2];
 };
 
 struct RowProgram {
@@ -705,21 +710,44 @@ __device__ __forceinline__ void rq_diag(C (&v)[16], const RowDiag& D, uint64_t r
   constexpr int M = 1 << LOGM, TPR = M / 16, IPS = 16 >> LOGC, Q = M >> LOGC, NC = 1 << LOGC;
   constexpr long long N = (long long)M << LOGC;
   const double2 rs = D.hasRowF ? eval_factor(D.rowF, rowBase) : make_double2(1.0, 0.0);
-  if (D.ftSign) {
-    // transform twiddles as running products from exact values (a thread's points
-    // are arithmetic progressions in n): T holds n = r + C (t + TPR w), S holds
-    // n = j1 M + r Q + t + TPR i at v[I j1 + i]
+  if (D.ftSign || D.nPl) {
+    // linear phases as running products from values at a thread's first point (a
+    // thread's points are arithmetic progressions in n): T holds
+    // n = r + C (t + TPR w), S holds n = j1 M + r Q + t + TPR i at v[I j1 + i].
+    // The transform twiddle's values are exact (integer-reduced angles).
+    double c = 0.0;
+    for (int k = 0; k < D.nPl; ++k)
+      c += (D.plCtrl[k] >= 0 && ((rowBase >> D.plCtrl[k]) & 1ull)) ? -D.plC[k] : D.plC[k];
+    c *= D.regDx;
+    auto at = [&](long long n) {
+      double2 f = D.ftSign ? ft_tw_at(n, N, D.ftSign) : make_double2(1.0, 0.0);
+      if (c != 0.0) {
+        double sn, cs;
+        sincos(c * ((double)n - D.regC), &sn, &cs);
+        f = dmul(f, make_double2(cs, sn));
+      }
+      return f;
+    };
+    auto ratio = [&](long long d) {
+      double2 f = D.ftSign ? ft_tw_ratio(d, N, D.ftSign) : make_double2(1.0, 0.0);
+      if (c != 0.0) {
+        double sn, cs;
+        sincos(c * (double)d, &sn, &cs);
+        f = dmul(f, make_double2(cs, sn));
+      }
+      return f;
+    };
     if (layoutT) {
-      double2 f = dmul(ft_tw_at(r + NC * t, N, D.ftSign), rs);
-      const double2 st = ft_tw_ratio((long long)NC * TPR, N, D.ftSign);
+      double2 f = dmul(at(r + NC * t), rs);
+      const double2 st = ratio((long long)NC * TPR);
 #pragma unroll
       for (int w = 0; w < 16; ++w) {
         v[w] = cmul(v[w], fromd<C>(f));
         f = dmul(f, st);
       }
     } else {
-      double2 f = dmul(ft_tw_at(r * Q + t, N, D.ftSign), rs);
-      const double2 si = ft_tw_ratio(TPR, N, D.ftSign), sj = ft_tw_ratio(M, N, D.ftSign);
+      double2 f = dmul(at(r * Q + t), rs);
+      const double2 si = ratio(TPR), sj = ratio(M);
 #pragma unroll
       for (int j1 = 0; j1 < NC; ++j1) {
         double2 g = f;
@@ -822,15 +850,14 @@ __device__ __forceinline__ void mbar_wait_bounded(uint32_t bar, uint32_t parity,
 // after every peer's arrival.
 template <typename C, int TPR, int LOGC>
 __device__ __forceinline__ void rq_exchange(C (&v)[16], C* buf, uint32_t bar, uint32_t& parity, int t, int r,
-                                            unsigned int* err) {
+                                            const uint32_t* peerBuf, const uint32_t* peerBar, unsigned int* err) {
   constexpr int NC = 1 << LOGC, IPS = 16 >> LOGC;
   if (t == 0) mbar_expect_tx(bar, (uint32_t)((16 - IPS) * TPR * sizeof(C)));
   cluster_wait_acquire();
-  const uint32_t base = smem_addr(buf), rbar = bar;
 #pragma unroll
   for (int q = 0; q < NC; ++q) {
     if (q == r) continue;
-    const uint32_t dst = cluster_map(base, q), dbar = cluster_map(rbar, q);
+    const uint32_t dst = peerBuf[q], dbar = peerBar[q];  // the peer's buffer and mbarrier
 #pragma unroll
     for (int i = 0; i < IPS; ++i)
       st_async(dst + (uint32_t)(((IPS * r + i) * TPR + t) * sizeof(C)), v[IPS * q + i], dbar);
@@ -879,7 +906,13 @@ __global__ void __launch_bounds__(1 << (LOGN - LOGC - 4), 1 << (LOGC - 1))
   const int t = threadIdx.x;
   const uint32_t bar = smem_addr(&xbar);
   uint32_t parity = 0;
+  // the peers' buffer and mbarrier addresses in the cluster window, mapped once
+  __shared__ uint32_t peerBuf[NC], peerBar[NC];
   if (t == 0) mbar_init(bar, 1);
+  if (t < NC) {
+    peerBuf[t] = cluster_map(smem_addr(sm), t);
+    peerBar[t] = cluster_map(bar, t);
+  }
   {
     const int scM = P.logTwN - LOGM, scN = P.logTwN - LOGN;
     constexpr int NTAB = 2 * (64 + (M >> 6));
@@ -929,14 +962,14 @@ __global__ void __launch_bounds__(1 << (LOGN - LOGC - 4), 1 << (LOGC - 1))
 #pragma unroll
         for (int i = 0; i < IPS; ++i) rq_cross<C, 1, LOGC>(v, i, loN, hiN, r * Q + t + TPR * i);
         if (!arrived) cluster_arrive_release();  // this CTA is done with its buffer
-        rq_exchange<C, TPR, LOGC>(v, sm, bar, parity, t, r, P.waitErr);
+        rq_exchange<C, TPR, LOGC>(v, sm, bar, parity, t, r, peerBuf, peerBar, P.waitErr);
         arrived = false;
         rr_stages<C, 1, LOGM, 0, 4>(v, sm, t, loM, hiM);
         layoutT = true;
       } else {  // T -> S
         rr_stages<C, -1, LOGM, 0, 4>(v, sm, t, loM, hiM);
         if (!arrived) cluster_arrive_release();
-        rq_exchange<C, TPR, LOGC>(v, sm, bar, parity, t, r, P.waitErr);
+        rq_exchange<C, TPR, LOGC>(v, sm, bar, parity, t, r, peerBuf, peerBar, P.waitErr);
         arrived = false;
 #pragma unroll
         for (int i = 0; i < IPS; ++i) rq_cross<C, -1, LOGC>(v, i, loN, hiN, r * Q + t + TPR * i);
@@ -1218,12 +1251,37 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
     D.tab = nullptr;
     D.permuted = opTransposed ? 1 : 0;
     D.ftSign = 0;
-    // on the cluster kernel a run of transform twiddles alone needs no table
-    bool twOnly = useC && !regTerms.empty() && bits.empty();
-    for (const Term& t : regTerms) twOnly &= t.kind == kTermFtTw;
-    if (twOnly) {
-      for (const Term& t : regTerms) D.ftSign += t.sign;
-      regTerms.clear();
+    D.nPl = 0;
+    // On the cluster kernel a run whose register terms are linear phases (transform
+    // twiddles, c x terms controlled by row bits) needs no table.
+    {
+      const int lo = ctx->flw[reg], hi = lo + q;
+      bool linOnly = useC && !regTerms.empty();
+      int nPl = 0;
+      for (const Term& t : regTerms) {
+        if (t.kind == kTermFtTw && t.ctrlBit < 0) continue;
+        const bool rowCtrl = t.ctrlBit < 0 || t.ctrlBit < lo || t.ctrlBit >= hi;
+        if (t.kind == kTermPoly && t.power == 1 && rowCtrl && nPl < 2) {
+          ++nPl;
+          continue;
+        }
+        linOnly = false;
+      }
+      if (linOnly) {
+        for (const Term& t : regTerms) {
+          if (t.kind == kTermFtTw) {
+            D.ftSign += t.sign;
+            continue;
+          }
+          D.plC[D.nPl] = t.coeff;
+          D.plCtrl[D.nPl++] = t.ctrlBit;
+        }
+        D.regC = (double)((1 << q) - 1) * 0.5;
+        D.regDx = ctx->dx[reg];
+        regTerms.clear();
+        bits.clear();
+        D.nCtrl = 0;
+      }
     }
     if (!regTerms.empty()) {
       double2* tab = (double2*)arena_alloc(ctx, ((size_t)1 << (q + D.nCtrl)) * sizeof(double2));
