@@ -967,8 +967,16 @@ __global__ void __launch_bounds__(1 << (LOGN - LOGC - 4), 1 << (LOGC - 1))
         rr_stages<C, 1, LOGM, 0, 4>(v, sm, t, loM, hiM);
         layoutT = true;
       } else {  // T -> S
-        rr_stages<C, -1, LOGM, 0, 4>(v, sm, t, loM, hiM);
-        if (!arrived) cluster_arrive_release();
+        // the buffer is free once the stages' last exchange is read: arrive there,
+        // so the last stage's butterflies overlap the peers' progress
+        if (!arrived) {
+          struct Arrive {
+            __device__ __forceinline__ void operator()() const { cluster_arrive_release(); }
+          };
+          rr_stages<C, -1, LOGM, 0, 4, Arrive>(v, sm, t, loM, hiM, Arrive());
+        } else {
+          rr_stages<C, -1, LOGM, 0, 4>(v, sm, t, loM, hiM);
+        }
         rq_exchange<C, TPR, LOGC>(v, sm, bar, parity, t, r, peerBuf, peerBar, P.waitErr);
         arrived = false;
 #pragma unroll

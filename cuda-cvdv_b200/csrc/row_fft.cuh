@@ -223,15 +223,21 @@ __device__ __forceinline__ void rr_exchange(C (&v)[1 << LOGE], C* smrow, int t) 
 // The stages of one transform: radix 16 (radix 32 with 32 amplitudes a thread,
 // radix 8 with 8), then the remaining radix.  The shared row holds at least
 // M + M/16 elements (M + M/8 with 8 amplitudes a thread).
-template <typename C, int DIR, int LOGM, int S, int LOGE = 4>
+// AFTER: a callable run once the shared row is no longer needed (after the last
+// exchange, before the last stage's butterflies)
+struct NoHook {
+  __device__ __forceinline__ void operator()() const {}
+};
+template <typename C, int DIR, int LOGM, int S, int LOGE = 4, typename H = NoHook>
 __device__ __forceinline__ void rr_stages(C (&v)[1 << LOGE], C* smrow, int t, const double2* lo,
-                                          const double2* hi) {
+                                          const double2* hi, H after = H()) {
   constexpr int LR = LOGE >= 5 ? 5 : (LOGE == 3 ? 3 : 4);  // log2 of the full stages' radix
   constexpr int NF = LOGM / LR, REM = LOGM % LR;
   if constexpr (S < NF) {
     rr_butterflies<C, DIR, LOGM, LR, LR * S, LOGE>(v, t, lo, hi);
     if constexpr (S + 1 < NF || REM) rr_exchange<C, LOGM, LR, LR * S, LOGE, LR>(v, smrow, t);
-    rr_stages<C, DIR, LOGM, S + 1, LOGE>(v, smrow, t, lo, hi);
+    if constexpr ((REM > 0 && S + 1 == NF) || (REM == 0 && S + 2 == NF)) after();
+    rr_stages<C, DIR, LOGM, S + 1, LOGE, H>(v, smrow, t, lo, hi, after);
   } else if constexpr (REM > 0) {
     rr_butterflies<C, DIR, LOGM, REM, LR * NF, LOGE>(v, t, lo, hi);
   }
