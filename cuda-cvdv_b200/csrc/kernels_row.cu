@@ -479,13 +479,34 @@ __global__ void __launch_bounds__(1 << LOGT, (LOGC > 0 || LOGT > 8) ? 1 : 2)
 // strides are template constants, so every shared-memory address is a
 // per-thread base plus an immediate offset.
 
+// exp(i pi s (N-1)(2n-N+1)/(2N)) with the angle reduced exactly in integers, and
+// its ratio between n + d and n, exp(i pi s (N-1) d / N)
+__device__ __forceinline__ double2 ft_tw_at(long long n, long long N, int s) {
+  long long m = ((N - 1) * (2 * n - N + 1) * s) % (4 * N);
+  if (m < 0) m += 4 * N;
+  double sn, c;
+  sincospi((double)m / (double)(2 * N), &sn, &c);
+  return make_double2(c, sn);
+}
+__device__ __forceinline__ double2 ft_tw_ratio(long long d, long long N, int s) {
+  long long m = ((N - 1) * d * s) % (2 * N);
+  if (m < 0) m += 2 * N;
+  double sn, c;
+  sincospi((double)m / (double)N, &sn, &c);
+  return make_double2(c, sn);
+}
+
 template <typename C, int LOGM, int LOGE>
 __device__ __forceinline__ void rr_diag(C (&v)[1 << LOGE], const RowDiag& D, uint64_t rowBase, int t) {
   constexpr int E = 1 << LOGE, TPR = 1 << (LOGM - LOGE);
   const double2 rs = D.hasRowF ? eval_factor(D.rowF, rowBase) : make_double2(1.0, 0.0);
   // running factor of element t + k TPR: rs times the linear phase, advanced by st per k
   double2 f = rs, st = make_double2(1.0, 0.0);
-  if (D.nLin) {
+  const bool lin = D.nLin || D.nPl || D.ftSign;
+  if (lin) {
+    // bilinear terms with other registers and c x terms (controls off the row) are
+    // one linear phase a (m - regC) regDx along the row; the transform twiddle is
+    // exact at the first point and as a ratio per step
     double a = 0.0;
     for (int l = 0; l < D.nLin; ++l) {
       const XXFactor& X = D.lin[l];
@@ -494,11 +515,17 @@ __device__ __forceinline__ void rr_diag(C (&v)[1 << LOGE], const RowDiag& D, uin
       if (X.ctrlShift >= 0 && ((rowBase >> X.ctrlShift) & 1ull)) c = -c;
       a += c;
     }
+    for (int k = 0; k < D.nPl; ++k)
+      a += (D.plCtrl[k] >= 0 && ((rowBase >> D.plCtrl[k]) & 1ull)) ? -D.plC[k] : D.plC[k];
     a *= D.regDx;
     double s0, c0;
     sincos(a * ((double)t - D.regC), &s0, &c0);
     sincos(a * (double)TPR, &st.y, &st.x);
     f = dmul(rs, make_double2(c0, s0));
+    if (D.ftSign) {
+      f = dmul(f, ft_tw_at(t, 1ll << LOGM, D.ftSign));
+      st = dmul(st, ft_tw_ratio(TPR, 1ll << LOGM, D.ftSign));
+    }
   }
   if (D.tab) {
     int seg = 0;
@@ -511,12 +538,12 @@ __device__ __forceinline__ void rr_diag(C (&v)[1 << LOGE], const RowDiag& D, uin
       for (int k = 0; k < 8; ++k) w[k] = __ldg(tp + (k0 + k) * TPR);
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
-        if (D.hasRowF || D.nLin) w[k] = dmul(w[k], f);
-        if (D.nLin) f = dmul(f, st);
+        if (D.hasRowF || lin) w[k] = dmul(w[k], f);
+        if (lin) f = dmul(f, st);
         v[k0 + k] = cmul(v[k0 + k], fromd<C>(w[k]));
       }
     }
-  } else if (D.nLin) {
+  } else if (lin) {
 #pragma unroll
     for (int k = 0; k < E; ++k) {
       v[k] = cmul(v[k], fromd<C>(f));
@@ -687,23 +714,6 @@ bool col_program_ok(Context* ctx, int reg) {
 // receiving CTA's shared memory (slot (I src + i) TPR + t); the I it keeps never
 // leave its registers.  Diagonal runs in T read tables stored permuted for C CTAs
 // (position r M + k2 holds index r + C k2).
-// exp(i pi s (N-1)(2n-N+1)/(2N)) with the angle reduced exactly in integers, and
-// its ratio between n + d and n, exp(i pi s (N-1) d / N)
-__device__ __forceinline__ double2 ft_tw_at(long long n, long long N, int s) {
-  long long m = ((N - 1) * (2 * n - N + 1) * s) % (4 * N);
-  if (m < 0) m += 4 * N;
-  double sn, c;
-  sincospi((double)m / (double)(2 * N), &sn, &c);
-  return make_double2(c, sn);
-}
-__device__ __forceinline__ double2 ft_tw_ratio(long long d, long long N, int s) {
-  long long m = ((N - 1) * d * s) % (2 * N);
-  if (m < 0) m += 2 * N;
-  double sn, c;
-  sincospi((double)m / (double)N, &sn, &c);
-  return make_double2(c, sn);
-}
-
 template <typename C, int LOGM, int LOGC>
 __device__ __forceinline__ void rq_diag(C (&v)[16], const RowDiag& D, uint64_t rowBase, int t, int r,
                                         bool layoutT) {
@@ -1264,7 +1274,7 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
     // twiddles, c x terms controlled by row bits) needs no table.
     {
       const int lo = ctx->flw[reg], hi = lo + q;
-      bool linOnly = useC && !regTerms.empty();
+      bool linOnly = (useC || toRowr) && !regTerms.empty();
       int nPl = 0;
       for (const Term& t : regTerms) {
         if (t.kind == kTermFtTw && t.ctrlBit < 0) continue;
