@@ -406,7 +406,8 @@ def run_gpu(args, world, rank, local):
                                          "like-for-like end-to-end figure",
                 "product_deferral": "gates queued after the separable init that act on the mode alone (the "
                                     "preparation and the first transform) run on the mode's 2^14 array before "
-                                    "the product state is formed",
+                                    "the product state is formed; the first qubit-gate sequence pass then forms "
+                                    "each amplitude from the product tables instead of reading a written product",
                 "value_product_deferral_off": G * world / e2e_nodefer_s},
         "norm_after": norm,
         "queue_fusion": "FtP2Q/FtQ2P pairs separated only by gates on other registers are cancelled "

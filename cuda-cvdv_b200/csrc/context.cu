@@ -653,19 +653,38 @@ static bool starts_blocked(Context* ctx, std::vector<Op>& ops, int r) {
 // that register's array is first put in the blocked order of a cluster of
 // C = 2^rowc_log_cluster() CTAs (position h M + k2 holds index h + C k2, M = N / C),
 // so the state comes out blocked in it.
-static bool launch_product(Context* ctx, std::vector<const double2*>& arrs, int blockedReg) {
-  bool ok = true;
-  if (blockedReg >= 0) {
-    const int nC = 1 << rowc_log_cluster();
-    const size_t M = ((size_t)1 << ctx->q[blockedReg]) / nC;
-    double2* t = (double2*)arena_alloc(ctx, nC * M * sizeof(double2));
-    ok = t != nullptr;
-    for (int h = 0; ok && h < nC; ++h)
-      ok = cuda_ok(ctx, cudaMemcpy2DAsync(t + h * M, sizeof(double2), arrs[blockedReg] + h, nC * sizeof(double2),
-                                          sizeof(double2), M, cudaMemcpyDeviceToDevice, ctx->stream),
-                   "blocked register array");
-    if (ok) arrs[blockedReg] = t;
+static bool blocked_array(Context* ctx, std::vector<const double2*>& arrs, int blockedReg) {
+  if (blockedReg < 0) return true;
+  const int nC = 1 << rowc_log_cluster();
+  const size_t M = ((size_t)1 << ctx->q[blockedReg]) / nC;
+  double2* t = (double2*)arena_alloc(ctx, nC * M * sizeof(double2));
+  bool ok = t != nullptr;
+  for (int h = 0; ok && h < nC; ++h)
+    ok = cuda_ok(ctx, cudaMemcpy2DAsync(t + h * M, sizeof(double2), arrs[blockedReg] + h, nC * sizeof(double2),
+                                        sizeof(double2), M, cudaMemcpyDeviceToDevice, ctx->stream),
+                 "blocked register array");
+  if (ok) arrs[blockedReg] = t;
+  return ok;
+}
+
+// The product formed by the flush's first qubit-gate sequence: only the tables
+// (the other registers' outer product, the last register's array) are made here.
+static bool product_tables(Context* ctx, std::vector<const double2*>& arrs, int blockedReg) {
+  const int R = ctx->numReg;
+  double2* outer = (double2*)arena_alloc(ctx, ((size_t)1 << (ctx->totalQbt - ctx->q[R - 1])) * sizeof(double2));
+  const bool ok = outer && blocked_array(ctx, arrs, blockedReg) && launch_outer(ctx, arrs.data(), outer);
+  ctx->productPending = false;
+  if (!ok) {
+    ctx->initialized = false;
+    return false;
   }
+  ctx->seqProdLast = arrs[R - 1];
+  ctx->seqProdOuter = outer;
+  return true;
+}
+
+static bool launch_product(Context* ctx, std::vector<const double2*>& arrs, int blockedReg) {
+  bool ok = blocked_array(ctx, arrs, blockedReg);
   ok = ok && launch_init_product(ctx, arrs.data());
   // The register arrays already carry the stages run on them and the rest of the
   // queue is dropped with the flush, so a product that could not be formed leaves
@@ -804,7 +823,10 @@ bool flush(Context* ctx) {
     // a first program on the last register that reads it blocked gets the product blocked
     const int last = ctx->numReg - 1;
     const int blocked = starts_blocked(ctx, ops, last) ? last : -1;
-    if (!launch_product(ctx, arrs, blocked)) return false;
+    // when the flush opens with a qubit-gate sequence, that pass forms the product
+    const bool inSeq = ctx->fuseSeq && ctx->numReg >= 2 && ops[0].st && ops[0].st->kind == kStPair &&
+                       seq_extent(ctx, ops, 0) >= 2;
+    if (!(inSeq ? product_tables(ctx, arrs, blocked) : launch_product(ctx, arrs, blocked))) return false;
     if (blocked >= 0) {
       ctx->permReg = blocked;
       ctx->permLogC = rowc_log_cluster();
@@ -823,7 +845,12 @@ bool flush(Context* ctx) {
           seq.push_back(std::move(p));
           if (!ops[k].post.empty()) seq.push_back({1, -1, {}, ops[k].post});
         }
-        if (!launch_seq(ctx, seq)) return false;
+        const bool forms = ctx->seqProdLast != nullptr;
+        if (!launch_seq(ctx, seq)) {
+          ctx->seqProdLast = ctx->seqProdOuter = nullptr;
+          if (forms) ctx->initialized = false;  // the product state was never written
+          return false;
+        }
         oi += ext - 1;
         continue;
       }

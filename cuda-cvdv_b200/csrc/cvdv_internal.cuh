@@ -284,6 +284,11 @@ struct Context {
   // over it are built permuted.
   int permReg = -1;
   int permLogC = 0;
+  // Inside one flush: the product state not yet written; the first qubit-gate
+  // sequence forms each amplitude as last[i mod N_last] * outer[i / N_last] from
+  // these tables instead of reading the state (set by flush, taken by launch_seq)
+  const double2* seqProdLast = nullptr;
+  const double2* seqProdOuter = nullptr;
   int nextFtTag = 1;
   long long ftCancelled = 0;
 

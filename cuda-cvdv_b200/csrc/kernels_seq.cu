@@ -51,6 +51,10 @@ struct SeqOp {
 
 struct SeqProgram {
   int bits[kSeqMaxBits];  // global bit positions, ascending
+  // the state is the product last[i mod 2^prodQ] * outer[i >> prodQ], formed here
+  const double2* prodLast;
+  const double2* prodOuter;
+  int prodQ;
   int nOps;
   SeqOp ops[kSeqMaxOps];
   SeqDiag diag[kSeqMaxDiags];
@@ -176,7 +180,11 @@ __device__ __forceinline__ void seq_pair_lanes(C* v, int kind, const Mat2 m, int
 // lane bit exchange partners with warp shuffles.  GEN = false: the sequence's 2x2
 // gates are all Hadamard-type, and the general-matrix paths are compiled out
 // (fewer live registers, fewer spills of the site).
-template <typename C, int NB, int SPLIT, typename IDX, bool GEN>
+//
+// PROD: the state is not written yet; each amplitude is formed from the product
+// tables (the register arrays' outer product and the last register's array), so
+// the product costs no pass of its own.
+template <typename C, int NB, int SPLIT, typename IDX, bool GEN, bool PROD>
 __global__ void __launch_bounds__(256, 2) k_seq(C* __restrict__ st, IDX nSites,
                                                const __grid_constant__ SeqProgram P) {
   constexpr int NBL = NB - SPLIT;  // bits held in registers
@@ -213,8 +221,17 @@ __global__ void __launch_bounds__(256, 2) k_seq(C* __restrict__ st, IDX nSites,
     // than held in KL registers across the site's gates
     const volatile IDX* vso = soff;
     C v[KL];
+    if constexpr (PROD) {
+      const IDX lm = ((IDX)1 << P.prodQ) - 1;
 #pragma unroll
-    for (int k = 0; k < KL; ++k) v[k] = st[base + hoff + vso[k]];
+      for (int k = 0; k < KL; ++k) {
+        const IDX a = base + hoff + vso[k];
+        v[k] = fromd<C>(dmul(__ldg(P.prodLast + (a & lm)), __ldg(P.prodOuter + (a >> P.prodQ))));
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < KL; ++k) v[k] = st[base + hoff + vso[k]];
+    }
     R sc = (R)1;  // pending real factor of Hadamard-type pairs
     for (int o = 0; o < P.nOps; ++o) {
       const SeqOp& op = P.ops[o];
@@ -334,8 +351,14 @@ template <typename C, int NB, int SPLIT, typename IDX>
 static void seq_go(Context* ctx, unsigned blocks, uint64_t nSites, const SeqProgram& P) {
   bool gen = false;
   for (int o = 0; o < P.nOps; ++o) gen |= P.ops[o].kind == kSeqPair || P.ops[o].kind == kSeqPairReal;
-  if (gen) k_seq<C, NB, SPLIT, IDX, true><<<blocks, 256, 0, ctx->stream>>>((C*)ctx->state(), (IDX)nSites, P);
-  else k_seq<C, NB, SPLIT, IDX, false><<<blocks, 256, 0, ctx->stream>>>((C*)ctx->state(), (IDX)nSites, P);
+  C* st = (C*)ctx->state();
+  if (P.prodLast) {
+    if (gen) k_seq<C, NB, SPLIT, IDX, true, true><<<blocks, 256, 0, ctx->stream>>>(st, (IDX)nSites, P);
+    else k_seq<C, NB, SPLIT, IDX, false, true><<<blocks, 256, 0, ctx->stream>>>(st, (IDX)nSites, P);
+  } else {
+    if (gen) k_seq<C, NB, SPLIT, IDX, true, false><<<blocks, 256, 0, ctx->stream>>>(st, (IDX)nSites, P);
+    else k_seq<C, NB, SPLIT, IDX, false, false><<<blocks, 256, 0, ctx->stream>>>(st, (IDX)nSites, P);
+  }
 }
 
 template <typename C, typename IDX>
@@ -367,6 +390,12 @@ bool launch_seq(Context* ctx, const std::vector<HostSeqOp>& ops) {
   }
   SeqProgram P{};
   for (int b = 0; b < nb; ++b) P.bits[b] = bits[b];
+  if (ctx->seqProdLast) {  // this pass forms the product state
+    P.prodLast = ctx->seqProdLast;
+    P.prodOuter = ctx->seqProdOuter;
+    P.prodQ = ctx->q[ctx->numReg - 1];
+    ctx->seqProdLast = ctx->seqProdOuter = nullptr;
+  }
   int nd = 0;
   for (const HostSeqOp& h : ops) {
     SeqOp& o = P.ops[P.nOps++];

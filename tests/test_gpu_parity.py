@@ -405,6 +405,36 @@ def test_state_transfer_scaled(n_qubits, mode_qubits):
             np.testing.assert_allclose(sim.m(k), o.m(k), atol=10 * tol)
 
 
+@pytest.mark.parametrize("n_qubits,mode_qubits", [(6, 12), (5, 14)])
+def test_product_formed_in_first_sequence(n_qubits, mode_qubits):
+    """With the product deferred and a qubit-gate sequence first in the flush, that
+    sequence forms each amplitude from the register arrays' product tables (one
+    outer-product launch, no product pass): equal to the oracle and to the run
+    with deferral off, in both precisions (the 2^14 mode also exercises the
+    blocked product)."""
+    from cvdv_b200 import CudaCvdv, _lib
+    from cvdv_b200 import workloads as W
+    circ = W.state_transfer(n_qubits=n_qubits, mode_qubits=mode_qubits)
+    o = OracleSim(circ["qubits"])
+    o.initStateVector(W.separable_arrays(circ))
+    W.apply(o, circ["prep"] + circ["gates"])
+    ref = o.get_state()
+    for prec, tol in (("complex128", PLAIN_TOL), ("complex64", MIXED_TOL)):
+        outs = {}
+        for flags in (31, 15):
+            sim = CudaCvdv(circ["qubits"], precision=prec, check_errors=True)
+            sim.setFusion(flags)
+            _lib.load().cvdvSetTiming(sim.ctx, 1)
+            sim.initStateVector(W.separable_arrays(circ, device="cuda"))
+            W.apply(sim, circ["prep"] + circ["gates"])
+            outs[flags] = sim.getState()
+            st = _lib.kernel_stats(sim.ctx)
+            if flags == 31:
+                assert st["init"][1] == 1 and st["seq"][1] >= 1, (prec, st)
+            assert rel(outs[flags], ref) < tol, (prec, flags, rel(outs[flags], ref))
+        assert rel(outs[31], outs[15]) < tol
+
+
 def test_transform_cancellation_matches_unfused():
     """Queue cancellation of FtP2Q/FtQ2P pairs changes nothing but rounding."""
     from cvdv_b200 import CudaCvdv, _lib
