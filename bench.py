@@ -325,7 +325,7 @@ def run_gpu(args, world, rank, local):
     # 2^24-amplitude version of this workload (profiles/*_state_transfer_2p24.md),
     # scaled by the 16x larger state: the kernels stream the state once per launch,
     # so their traffic grows with the rows / sites processed.
-    ncu_traffic_2p24 = {"fft_pass": ((269.3 + 221.1) + (269.0 + 220.7)) / 2 * 1e6,  # k_rowq, two launches
+    ncu_traffic_2p24 = {"fft_pass": ((268.6 + 218.8) + (268.6 + 218.6)) / 2 * 1e6,  # k_rowq, two launches
                         "seq": (270.4 + 212.4) * 1e6}                                  # k_seq<double2, 5, 1, u32, 0>
     scale = n_amp / float(1 << 24)
     traffic = ncu_traffic_2p24[dom] * scale if (dom in ncu_traffic_2p24 and args.workload == "full") else None
