@@ -717,6 +717,56 @@ def husimi_readout(args):
     return out
 
 
+def diagonal_runs(args):
+    """A standalone diagonal run on two modes [14, 14] (2^28 complex128 amplitudes;
+    [12, 12] for --workload small): a bilinear phase, a shear and a cubic phase that
+    no transform, sequence or row program absorbs run as one k_diag pass (each
+    register's phases from one table, the bilinear term's sincos per amplitude)."""
+    import torch
+    from cvdv_b200 import CudaCvdv, _lib
+    from cvdv_b200.separable import SeparableState
+    L = _lib.load()
+    mq = 14 if args.workload == "full" else 12
+    sep = SeparableState([mq, mq])
+    sep.setCoherent(0, 0.5 + 0.2j)
+    sep.setFock(1, 1)
+    sim = CudaCvdv([mq, mq], check_errors=True)
+    sim.initStateVector(sep)
+
+    def run():
+        sim.q1q2(0, 1, 0.1)
+        sim.sheer(0, 0.05)
+        sim.phaseCubic(1, 0.01)
+        L.cvdvFlush(sim.ctx)
+
+    run()
+    sim.synchronize()
+    stream = torch.cuda.ExternalStream(L.cvdvGetStream(sim.ctx))
+    reps = max(3, min(args.steps, 10))
+    for _ in range(args.warmup):
+        run()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        run()
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    L.cvdvSetTiming(sim.ctx, 1)
+    _lib.kernel_stats(sim.ctx)
+    run()
+    st = _lib.kernel_stats(sim.ctx)
+    L.cvdvSetTiming(sim.ctx, 0)
+    state_bytes = 16 << (2 * mq)
+    diag_ms, n = st["diag"]
+    out = {"unit": "ms", "amplitudes": 1 << (2 * mq), "ms_per_run": ms, "diag_launches": n,
+           "table_builds": st["table"][1], "table_ms": st["table"][0],
+           "achieved_gbs": 2 * state_bytes / (diag_ms / max(n, 1) * 1e-3) / 1e9 if n else None}
+    del sim
+    torch.cuda.empty_cache()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -731,7 +781,7 @@ def main():
     ap.add_argument("--workload", default="full", choices=["full", "small"],
                     help="small: 10 qubit registers + the 2^14 mode (2^24 amplitudes), and the two-mode "
                          "network at [12, 12], for ncu")
-    ap.add_argument("--extra", default=None, choices=["c3", "c4", "c5", "husimi"],
+    ap.add_argument("--extra", default=None, choices=["c3", "c4", "c5", "husimi", "diag"],
                     help="run only that extra measurement (one GPU) and print its JSON, for profiling")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -739,7 +789,8 @@ def main():
     world, rank, local = dist_init()
     try:
         if args.extra:
-            fn = {"c3": gaussian_c3, "c4": batched_c4, "c5": variational_c5, "husimi": husimi_readout}[args.extra]
+            fn = {"c3": gaussian_c3, "c4": batched_c4, "c5": variational_c5, "husimi": husimi_readout,
+                  "diag": diagonal_runs}[args.extra]
             print(json.dumps({"extra": args.extra, **fn(args)}), flush=True)
         elif args.impl == "reference":
             run_reference(args, world, rank)
