@@ -107,9 +107,16 @@ struct OpSep {  // sum conj(psi) * outer[i >> qLast] * last[i & m]   (measure.cu
 template <typename Op>
 __global__ void __launch_bounds__(kRedThreads) k_reduce(Op op, uint64_t n, double2* part) {
   double2 a = make_double2(0.0, 0.0);
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (uint64_t)gridDim.x * blockDim.x) {
-    double2 v = op(i);
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  // four terms evaluated before they are added, so four loads are in flight
+  for (; i + 3 * stride < n; i += 4 * stride) {
+    const double2 v0 = op(i), v1 = op(i + stride), v2 = op(i + 2 * stride), v3 = op(i + 3 * stride);
+    a.x += (v0.x + v1.x) + (v2.x + v3.x);
+    a.y += (v0.y + v1.y) + (v2.y + v3.y);
+  }
+  for (; i < n; i += stride) {
+    const double2 v = op(i);
     a.x += v.x;
     a.y += v.y;
   }
