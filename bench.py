@@ -676,8 +676,9 @@ def variational_c5(args):
     fd_err = {prec: float((grad_of(prec) - fd).abs().max()) / scale for prec in ("complex128", "complex64")}
     return {"value": 64 / (ms * 1e-3), "unit": "parameter-set gradients/s", "ms_per_step": ms,
             "batch": 64, "params_per_set": 80, "layout": [1, 12], "dtype": "c64",
-            "step": "forward (80 gates) + overlap + adjoint sweep (80 fused gradient/inverse steps), checkpoints "
-                    "every 16 gates; both sweeps replayed from CUDA graphs",
+            "step": "forward (80 gates as 40 fused Rx + cd layers) + overlap + adjoint sweep (40 fused layers: "
+                    "both gradients and the inverse gates), checkpoints every 16 gates; both sweeps replayed from "
+                    "CUDA graphs",
             "eager": {"value": 64 / (ms_eager * 1e-3), "ms_per_step": ms_eager,
                       "how": "the same step launching kernel by kernel from Python"},
             "adjoint_vs_central_differences": {"h": h, "max_rel_err": fd_err, "target": 1e-6,

@@ -20,11 +20,15 @@
 // states: G = -X/2 for Rx, and <lambda|K_cd|psi> = <F lambda| K |F psi> (F =
 // FtQ2P) for cd, taken between the two transforms.
 
+#include <cooperative_groups.h>
+
 #include <cmath>
 
 #include "../../include/cvdv.h"
 #include "cvdv_internal.cuh"
 #include "row_fft.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace cvdv {
 
@@ -316,6 +320,208 @@ __global__ void __launch_bounds__(BRow<LOGQ>::NT, 1)
     part[((uint64_t)blockIdx.x << G::LOGR) + tid] = racc[tid];
 }
 
+// ---------------------------------------------------------------- Rx then cd, fused
+// A layer Rx(theta) on qubit bit q followed by cd(beta) controlled by the same bit
+// runs as one pass: a cluster of two CTAs holds the two rows (mode arrays) that
+// differ only in that bit, CTA rank = the bit's value.  Each loads its row, the
+// Rx mixes it with the partner's row read from the partner's shared memory, and
+// the cd runs on the row in registers.  Rows of 2^9 .. 2^12 points, one CTA each.
+template <int LOGQ>
+struct BPair {
+  static constexpr int N = 1 << LOGQ, TPR = N >> 4, RS = N + (N >> 4);
+};
+
+// the row of cluster rank r for pair index p: the bit at position rb of the row
+// index (the qubit bit above the mode) set to r
+__device__ __forceinline__ uint64_t pair_row(uint64_t p, int rb, int r) {
+  return ((p >> rb) << (rb + 1)) | (p & ((1ull << rb) - 1)) | ((uint64_t)r << rb);
+}
+
+template <typename C, int LOGQ>
+__global__ void __launch_bounds__(BPair<LOGQ>::TPR, 1)
+    k_b_rxcd(C* __restrict__ st, int n, int bit, const double* __restrict__ th, const double* __restrict__ beta) {
+  using G = BPair<LOGQ>;
+  constexpr int N = G::N, TPR = G::TPR;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* sm = reinterpret_cast<C*>(smraw);
+  double2* lo = reinterpret_cast<double2*>(sm + G::RS);
+  double2* hi = lo + 64;
+  cg::cluster_group cl = cg::this_cluster();
+  const int r = (int)cl.block_rank(), t = threadIdx.x;
+  const uint64_t rowBase = pair_row(blockIdx.x >> 1, bit - LOGQ, r) << LOGQ;
+  const uint64_t b = rowBase >> n;
+  b_fill_twiddles<LOGQ>(lo, t, TPR);
+  C v[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = st[rowBase + t + k * TPR];
+  // Rx: v <- c v - i s w with w the partner row's amplitude at the same point
+  // ([[c, -i s], [-i s, c]] is symmetric in the two rows)
+#pragma unroll
+  for (int k = 0; k < 16; ++k) sm[t + k * TPR] = v[k];
+  cl.sync();
+  {
+    const C* pw = cl.map_shared_rank(sm, r ^ 1);
+    double s, c;
+    sincos(0.5 * __ldg(th + b), &s, &c);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const double2 x = tod_b(v[k]), y = tod_b(pw[t + k * TPR]);
+      v[k] = fromd<C>(make_double2(c * x.x + s * y.y, c * x.y - s * y.x));
+    }
+  }
+  cl.sync();  // the partner has read this CTA's row before the stages reuse the buffer
+  // cd controlled by the bit (value r): as k_b_cd
+  const double coef = __ldg(beta + b) * (-M_SQRT2) * (r ? -1.0 : 1.0);
+  const double2 tw0 = ft_twiddle(t, N, 1), tws = ft_twiddle_step(TPR, N, 1);
+  double2 f = tw0;
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    v[k] = cmul(v[k], fromd<C>(f));
+    f = dmul(f, tws);
+  }
+  rr_stages<C, 1, LOGQ, 0, 4>(v, sm, t, lo, hi);
+  f = b_kick(t, N, coef);
+  const double2 ks = b_kick_step(TPR, N, coef);
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    v[k] = cmul(v[k], fromd<C>(f));
+    f = dmul(f, ks);
+  }
+  rr_stages<C, -1, LOGQ, 0, 4>(v, sm, t, lo, hi);
+  f = cconj(tw0);
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    st[rowBase + t + k * TPR] = cmul(v[k], fromd<C>(f));
+    f = dmul(f, cconj(tws));
+  }
+}
+
+// Adjoint of the fused layer, walked backwards: the cd's g_cd = <F lambda| K |F psi>
+// and cd^+ on both states (as k_b_cd_adj), then the Rx's
+// g_rx = <lambda| (-X/2) |psi> and Rx(-theta) on both, the partner rows read from
+// the partner's shared memory.  One partial of each per row.
+// With a single qubit bit above the mode (one cluster per instance) the cluster
+// adds its two rows' partials itself and writes gCd / gRx (partCd, partRx null).
+template <typename C, int LOGQ>
+__global__ void __launch_bounds__(BPair<LOGQ>::TPR, 1)
+    k_b_cdrx_adj(C* __restrict__ psi, C* __restrict__ lam, int n, int bit, const double* __restrict__ th,
+                 const double* __restrict__ beta, double2* __restrict__ partCd, double2* __restrict__ partRx,
+                 double* __restrict__ gCd, double* __restrict__ gRx) {
+  __shared__ double2 sums[2];  // this row's g_cd and g_rx
+  using G = BPair<LOGQ>;
+  constexpr int N = G::N, TPR = G::TPR;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* sm = reinterpret_cast<C*>(smraw);
+  C* keep = sm + G::RS;  // the transformed psi row, then psi after cd^+
+  C* park = keep + N;    // lambda after cd^+
+  double2* lo = reinterpret_cast<double2*>(park + N);
+  double2* hi = lo + 64;
+  cg::cluster_group cl = cg::this_cluster();
+  const int r = (int)cl.block_rank(), t = threadIdx.x;
+  const uint64_t row = pair_row(blockIdx.x >> 1, bit - LOGQ, r);
+  const uint64_t rowBase = row << LOGQ;
+  const uint64_t b = rowBase >> n;
+  const double kz = -M_SQRT2 * (r ? -1.0 : 1.0);  // K_k = kz x_k
+  const double coef = -__ldg(beta + b) * kz;       // exp(-i beta K)
+  const double dx = sqrt(2.0 * M_PI / (double)N);
+  b_fill_twiddles<LOGQ>(lo, t, TPR);
+  const double2 tw0 = ft_twiddle(t, N, 1), tws = ft_twiddle_step(TPR, N, 1);
+  C v[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = psi[rowBase + t + k * TPR];
+  double2 f = tw0;
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    v[k] = cmul(v[k], fromd<C>(f));
+    f = dmul(f, tws);
+  }
+  __syncthreads();
+  rr_stages<C, 1, LOGQ, 0, 4>(v, sm, t, lo, hi);
+#pragma unroll
+  for (int k = 0; k < 16; ++k) keep[t + k * TPR] = v[k];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = lam[rowBase + t + k * TPR];
+  f = tw0;
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    v[k] = cmul(v[k], fromd<C>(f));
+    f = dmul(f, tws);
+  }
+  rr_stages<C, 1, LOGQ, 0, 4>(v, sm, t, lo, hi);
+  double gx = 0.0, gy = 0.0;
+  f = b_kick(t, N, coef);
+  const double2 ks = b_kick_step(TPR, N, coef);
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    const int kk = t + k * TPR;
+    const double2 P = tod_b(keep[kk]), L = tod_b(v[k]);
+    const double w = kz * ((double)kk - 0.5 * (double)(N - 1)) * dx / (double)N;
+    gx += w * (L.x * P.x + L.y * P.y);
+    gy += w * (L.x * P.y - L.y * P.x);
+    const C fc = fromd<C>(f);
+    v[k] = cmul(v[k], fc);
+    keep[kk] = cmul(keep[kk], fc);
+    f = dmul(f, ks);
+  }
+  rr_stages<C, -1, LOGQ, 0, 4>(v, sm, t, lo, hi);
+  f = cconj(tw0);
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    park[t + k * TPR] = cmul(v[k], fromd<C>(f));
+    f = dmul(f, cconj(tws));
+  }
+#pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = keep[t + k * TPR];
+  rr_stages<C, -1, LOGQ, 0, 4>(v, sm, t, lo, hi);
+  f = cconj(tw0);
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    keep[t + k * TPR] = cmul(v[k], fromd<C>(f));
+    f = dmul(f, cconj(tws));
+  }
+  // this row's g_cd
+  {
+    const double2 g = block_sum2_b(make_double2(gx, gy));
+    if (t == 0) {
+      sums[0] = g;
+      if (partCd) partCd[row] = g;
+    }
+  }
+  cl.sync();  // both rows of the pair are in shared memory (psi in keep, lambda in park)
+  // Rx(-theta) and this row's half of g_rx = sum conj(l_r) (-p_{1-r} / 2)
+  {
+    const C* pk = cl.map_shared_rank(keep, r ^ 1);
+    const C* pp = cl.map_shared_rank(park, r ^ 1);
+    double s, co;
+    sincos(-0.5 * __ldg(th + b), &s, &co);
+    gx = gy = 0.0;
+#pragma unroll 4
+    for (int k = 0; k < 16; ++k) {
+      const int kk = t + k * TPR;
+      const double2 p0 = tod_b(keep[kk]), p1 = tod_b(pk[kk]);
+      const double2 l0 = tod_b(park[kk]), l1 = tod_b(pp[kk]);
+      gx -= 0.5 * (l0.x * p1.x + l0.y * p1.y);
+      gy -= 0.5 * (l0.x * p1.y - l0.y * p1.x);
+      psi[rowBase + kk] = fromd<C>(make_double2(co * p0.x + s * p1.y, co * p0.y - s * p1.x));
+      lam[rowBase + kk] = fromd<C>(make_double2(co * l0.x + s * l1.y, co * l0.y - s * l1.x));
+    }
+    const double2 g = block_sum2_b(make_double2(gx, gy));
+    if (t == 0) {
+      sums[1] = g;
+      if (partRx) partRx[row] = g;
+    }
+  }
+  cl.sync();  // both rows' sums are in shared memory; no CTA leaves while its partner reads it
+  if (!partCd && r == 0 && t < 2) {
+    const double2* ps = cl.map_shared_rank(sums, 1);
+    const double2 a = sums[t], c = ps[t];
+    double* out = t == 0 ? gCd : gRx;
+    out[2 * b] = a.x + c.x;
+    out[2 * b + 1] = a.y + c.y;
+  }
+  cl.sync();
+}
+
 // <t| a_b> per CTA chunk (t shared by every instance when tStride == 0)
 template <typename C>
 __global__ void __launch_bounds__(kBatchThreads) k_b_dot(const C* __restrict__ a, const C* __restrict__ tg,
@@ -431,11 +637,148 @@ static bool b_finish(const char* fn, double2* part, int per, int batch, double* 
   return ok;
 }
 
+// the fused layer: rows of 2^9 .. 2^12 points, a cluster of two CTAs per row pair
+template <typename C, int LOGQ>
+static cudaError_t b_rxcd_t(void* st, void* lam, int batch, int n, int bit, const double* th, const double* beta,
+                            double2* partCd, double2* partRx, double* gCd, double* gRx, cudaStream_t s) {
+  using G = BPair<LOGQ>;
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)((uint64_t)batch << (n - LOGQ)));
+  cfg.blockDim = dim3(G::TPR);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const size_t tw = (64 + (G::N >> 6)) * sizeof(double2);
+  if (!lam) {
+    cfg.dynamicSmemBytes = (size_t)G::RS * sizeof(C) + tw;
+    auto kern = k_b_rxcd<C, LOGQ>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.dynamicSmemBytes);
+    if (e != cudaSuccess) return e;
+    return cudaLaunchKernelEx(&cfg, kern, (C*)st, n, bit, th, beta);
+  }
+  cfg.dynamicSmemBytes = (size_t)(G::RS + 2 * G::N) * sizeof(C) + tw;
+  auto kern = k_b_cdrx_adj<C, LOGQ>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.dynamicSmemBytes);
+  if (e != cudaSuccess) return e;
+  return cudaLaunchKernelEx(&cfg, kern, (C*)st, (C*)lam, n, bit, th, beta, partCd, partRx, gCd, gRx);
+}
+
+template <typename C>
+static cudaError_t b_rxcd(void* st, void* lam, int batch, int n, int q, int bit, const double* th,
+                          const double* beta, double2* partCd, double2* partRx, double* gCd, double* gRx,
+                          cudaStream_t s) {
+  switch (q) {
+    case 9: return b_rxcd_t<C, 9>(st, lam, batch, n, bit, th, beta, partCd, partRx, gCd, gRx, s);
+    case 10: return b_rxcd_t<C, 10>(st, lam, batch, n, bit, th, beta, partCd, partRx, gCd, gRx, s);
+    case 11: return b_rxcd_t<C, 11>(st, lam, batch, n, bit, th, beta, partCd, partRx, gCd, gRx, s);
+    case 12: return b_rxcd_t<C, 12>(st, lam, batch, n, bit, th, beta, partCd, partRx, gCd, gRx, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+static bool b_rxcd_args(const char* fn, int n, int q, int bit) {
+  if (q < 9 || q > 12 || q >= n || bit < q || bit >= n) {
+    set_error(nullptr, kErrInvalidArg,
+              "%s: the mode must be the last register with 9..12 qubits and the qubit a bit above it", fn);
+    return false;
+  }
+  return true;
+}
+
 }  // namespace cvdv
 
 using namespace cvdv;
 
 extern "C" {
+
+int cvdvBatchRxCondDisp(void* states, int precision, int batch, int n, int modeQubits, int bit,
+                        const double* thetas, const double* betas, void* stream) {
+  const char* fn = "cvdvBatchRxCondDisp";
+  if (!b_check(fn, states, precision, batch, n) || !b_rxcd_args(fn, n, modeQubits, bit)) return kErrInvalidArg;
+  if (!thetas || !betas) {
+    set_error(nullptr, kErrInvalidArg, "%s: null angles or displacements", fn);
+    return kErrInvalidArg;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e;
+  {
+    LaunchScope _ls(nullptr, kKFft);
+    e = precision == kC128 ? b_rxcd<double2>(states, nullptr, batch, n, modeQubits, bit, thetas, betas, nullptr,
+                                             nullptr, nullptr, nullptr, s)
+                           : b_rxcd<float2>(states, nullptr, batch, n, modeQubits, bit, thetas, betas, nullptr,
+                                            nullptr, nullptr, nullptr, s);
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_error(nullptr, kErrCuda, "%s: %s", fn, cudaGetErrorString(e));
+    return kErrCuda;
+  }
+  return kOk;
+}
+
+int cvdvBatchRxCondDispAdjoint(void* psi, void* lam, int precision, int batch, int n, int modeQubits, int bit,
+                               const double* thetas, const double* betas, double* gRx, double* gCd,
+                               void* stream) {
+  const char* fn = "cvdvBatchRxCondDispAdjoint";
+  if (!b_check(fn, psi, precision, batch, n) || !b_rxcd_args(fn, n, modeQubits, bit)) return kErrInvalidArg;
+  if (!lam || !thetas || !betas || !gRx || !gCd) {
+    set_error(nullptr, kErrInvalidArg, "%s: null argument", fn);
+    return kErrInvalidArg;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  const int per = 1 << (n - modeQubits);  // rows per instance, one partial of each kind per row
+  if (per == 2) {  // one cluster per instance: it writes the sums itself
+    cudaError_t e;
+    {
+      LaunchScope _ls(nullptr, kKFft);
+      e = precision == kC128 ? b_rxcd<double2>(psi, lam, batch, n, modeQubits, bit, thetas, betas, nullptr,
+                                               nullptr, gCd, gRx, s)
+                             : b_rxcd<float2>(psi, lam, batch, n, modeQubits, bit, thetas, betas, nullptr,
+                                              nullptr, gCd, gRx, s);
+    }
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      set_error(nullptr, kErrCuda, "%s: %s", fn, cudaGetErrorString(e));
+      return kErrCuda;
+    }
+    return kOk;
+  }
+  const size_t np = (size_t)batch * per;
+  double2* part = nullptr;
+  if (cudaMallocAsync((void**)&part, 2 * np * sizeof(double2), s) != cudaSuccess) {
+    cudaGetLastError();
+    set_error(nullptr, kErrAlloc, "%s: partial sums", fn);
+    return kErrAlloc;
+  }
+  cudaError_t e;
+  {
+    LaunchScope _ls(nullptr, kKFft);
+    e = precision == kC128 ? b_rxcd<double2>(psi, lam, batch, n, modeQubits, bit, thetas, betas, part, part + np,
+                                             nullptr, nullptr, s)
+                           : b_rxcd<float2>(psi, lam, batch, n, modeQubits, bit, thetas, betas, part, part + np,
+                                            nullptr, nullptr, s);
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_error(nullptr, kErrCuda, "%s: %s", fn, cudaGetErrorString(e));
+    cudaFreeAsync(part, s);
+    return kErrCuda;
+  }
+  {
+    LaunchScope _ls(nullptr, kKReduce);
+    k_b_sum<<<(batch + 255) / 256, 256, 0, s>>>(part, per, batch, gCd);
+    k_b_sum<<<(batch + 255) / 256, 256, 0, s>>>(part + np, per, batch, gRx);
+  }
+  const bool ok = b_launch_ok(fn);
+  cudaFreeAsync(part, s);
+  return ok ? kOk : kErrCuda;
+}
+
 
 int cvdvBatchRx(void* states, int precision, int batch, int n, int bit, const double* thetas, double sign,
                 void* stream) {

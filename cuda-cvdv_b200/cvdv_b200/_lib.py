@@ -77,6 +77,10 @@ SIGNATURES = [
     ("cvdvBatchRxAdjoint", [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p], c_int),
     ("cvdvBatchCondDispAdjoint",
      [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p], c_int),
+    ("cvdvBatchRxCondDisp", [c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p], c_int),
+    ("cvdvBatchRxCondDispAdjoint",
+     [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p],
+     c_int),
     ("cvdvBatchOverlap", [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_void_p], c_int),
     ("cvdvBatchStructSizes", [POINTER(c_int)], None),
     ("cvdvBatchRunStage", [c_void_p, c_int, c_void_p, c_int, c_void_p, c_int, c_void_p], c_int),

@@ -15,8 +15,8 @@ to the final state and to the back-propagated target and reading
 ``g = <lambda|G|psi>`` for the gate's generator G on the way -- with the
 forward states recovered by the inverse gates, not stored, and reset from a
 checkpoint every ``checkpoint_every`` gates to bound the drift.  Each step is
-one kernel over the whole batch (libcvdv ``cvdvBatch*``); there is no CPU
-fallback.  With ``graphs=True`` both sweeps are captured in CUDA graphs once per
+one kernel over the whole batch (libcvdv ``cvdvBatch*``; an Rx followed by a cd
+controlled by the same qubit is one fused step); there is no CPU fallback.  With ``graphs=True`` both sweeps are captured in CUDA graphs once per
 shape and replayed (the per-gate launch and Python overhead dominate at the
 configured sizes).
 
@@ -76,6 +76,18 @@ class VariationalCircuit:
             else:
                 raise ValueError(f"unsupported gate {kind!r}")
         self._L = _lib.load()
+        # An Rx followed by a cd controlled by the same qubit runs as one fused layer
+        # (cvdvBatchRxCondDisp) when no checkpoint falls between the two: the steps
+        # are (first gate, number of gates) in circuit order.
+        q = self.qubits[self.mode]
+        self._steps: List[Tuple[int, int]] = []
+        g = 0
+        while g < len(self._gates):
+            pair = (g + 1 < len(self._gates) and self._gates[g][0] == "rx" and self._gates[g + 1][0] == "cd"
+                    and self._gates[g][1] == self._gates[g + 1][1] and 9 <= q <= 12
+                    and (g + 1) % self.checkpoint_every != 0)
+            self._steps.append((g, 2 if pair else 1))
+            g += 2 if pair else 1
 
     @property
     def n_gates(self) -> int:
@@ -94,10 +106,35 @@ class VariationalCircuit:
             _check(self._L.cvdvBatchCondDisp(_ptr(psi), self.prec, B, self.n, self.qubits[self.mode], bit,
                                              _ptr(p), sign, self._stream()))
 
-    def _adjoint(self, psi: torch.Tensor, lam: torch.Tensor, g: int, p: torch.Tensor) -> torch.Tensor:
+    def _apply_step(self, psi: torch.Tensor, g: int, n: int, p: torch.Tensor) -> None:
+        """Gates g .. g + n - 1 (n = 2: the fused Rx + cd layer)."""
+        if n == 1:
+            self._apply(psi, g, p[g])
+            return
+        _check(self._L.cvdvBatchRxCondDisp(_ptr(psi), self.prec, psi.shape[0], self.n, self.qubits[self.mode],
+                                           self._gates[g][1], _ptr(p[g]), _ptr(p[g + 1]), self._stream()))
+
+    def _adjoint_step(self, psi: torch.Tensor, lam: torch.Tensor, g: int, n: int, p: torch.Tensor,
+                      gvals: torch.Tensor) -> None:
+        """Adjoint of gates g + n - 1 .. g, writing their g values into gvals[g ...]."""
+        if n == 1:
+            self._adjoint(psi, lam, g, p[g], gvals[g])
+            return
+        grx = torch.view_as_real(gvals[g]).view(-1)
+        gcd = torch.view_as_real(gvals[g + 1]).view(-1)
+        _check(self._L.cvdvBatchRxCondDispAdjoint(_ptr(psi), _ptr(lam), self.prec, psi.shape[0], self.n,
+                                                  self.qubits[self.mode], self._gates[g][1], _ptr(p[g]),
+                                                  _ptr(p[g + 1]), _ptr(grx), _ptr(gcd), self._stream()))
+
+    def _adjoint(self, psi: torch.Tensor, lam: torch.Tensor, g: int, p: torch.Tensor,
+                 out: torch.Tensor = None) -> torch.Tensor:
+        """g_b = <lambda_b|G|psi_b> for every instance into `out` (complex128, (B,)), with
+        the gate's inverse applied to both states."""
         kind, bit = self._gates[g]
         B = psi.shape[0]
-        out = torch.empty(2 * B, dtype=torch.float64, device=psi.device)
+        if out is None:
+            out = torch.empty(B, dtype=torch.complex128, device=psi.device)
+        out = torch.view_as_real(out).view(-1)
         if kind == "rx":
             _check(self._L.cvdvBatchRxAdjoint(_ptr(psi), _ptr(lam), self.prec, B, self.n, bit, _ptr(p),
                                               _ptr(out), self._stream()))
@@ -131,8 +168,8 @@ class VariationalCircuit:
     def states(self, params: torch.Tensor, psi0: torch.Tensor) -> torch.Tensor:
         """Final states (batch, 2^n) for every parameter set; psi0 is one state or one per instance."""
         p, psi = self._prepare(params, psi0)
-        for g in range(self.n_gates):
-            self._apply(psi, g, p[g])
+        for g, n in self._steps:
+            self._apply_step(psi, g, n, p)
         return psi
 
     def fidelity_loss(self, params: torch.Tensor, psi0: torch.Tensor, target: torch.Tensor) -> torch.Tensor:
@@ -157,10 +194,10 @@ class _FidelityLoss(torch.autograd.Function):
         p, psi = circ._prepare(params, psi0)
         tgt = target.to(device="cuda", dtype=circ.cdtype).contiguous()
         checkpoints = {}
-        for g in range(circ.n_gates):
+        for g, n in circ._steps:
             if g % circ.checkpoint_every == 0 and g > 0:
                 checkpoints[g] = psi.clone()  # the state before gate g
-            circ._apply(psi, g, p[g])
+            circ._apply_step(psi, g, n, p)
         ov = circ._overlap(psi, tgt)
         ctx.circ = circ
         ctx.checkpoints = checkpoints
@@ -175,14 +212,14 @@ class _FidelityLoss(torch.autograd.Function):
         B = psi_final.shape[0]
         psi = psi_final.clone()
         lam = tgt.expand(B, -1).contiguous() if tgt.dim() == 1 else tgt.clone()
-        grads = torch.empty(circ.n_gates, B, dtype=torch.float64, device=psi.device)
-        for g in reversed(range(circ.n_gates)):
-            gval = circ._adjoint(psi, lam, g, p[g])
-            # dL/dp = -2 Re(conj(ov) i <lam|G|psi>) = 2 Im(conj(ov) g)
-            grads[g] = 2.0 * (ov.conj() * gval).imag
+        gvals = torch.empty(circ.n_gates, B, dtype=torch.complex128, device=psi.device)
+        for g, n in reversed(circ._steps):
+            circ._adjoint_step(psi, lam, g, n, p, gvals)
             ck = ctx.checkpoints.get(g)
             if ck is not None:
                 psi.copy_(ck)
+        # dL/dp = -2 Re(conj(ov) i <lam|G|psi>) = 2 Im(conj(ov) g), every gate at once
+        grads = 2.0 * (ov.conj()[None, :] * gvals).imag
         gl = grad_loss.to(device=psi.device, dtype=torch.float64)
         return (grads.t() * gl[:, None]).to(ctx.params_device), None, None, None
 
@@ -203,6 +240,7 @@ class _GraphPlan:
         self.ck = {g: torch.empty_like(self.psi)
                    for g in range(circ.checkpoint_every, circ.n_gates, circ.checkpoint_every)}
         self.grads = torch.empty(circ.n_gates, B, dtype=torch.float64, device=dev)
+        self.gvals = torch.empty(circ.n_gates, B, dtype=torch.complex128, device=dev)
         self.generation = 0
         # one eager run of each sweep on a side stream (first-use set-up), then capture
         side = torch.cuda.Stream()
@@ -221,22 +259,22 @@ class _GraphPlan:
     def _forward(self) -> None:
         c = self.circ
         self.psi.copy_(self.psi0.expand_as(self.psi))
-        for g in range(c.n_gates):
+        for g, n in c._steps:
             if g in self.ck:
                 self.ck[g].copy_(self.psi)  # the state before gate g
-            c._apply(self.psi, g, self.p[g])
+            c._apply_step(self.psi, g, n, self.p)
         self.ov = c._overlap(self.psi, self.tgt)
 
     def _backward(self) -> None:
         c = self.circ
         self.back.copy_(self.psi)
         self.lam.copy_(self.tgt.expand_as(self.lam))
-        for g in reversed(range(c.n_gates)):
-            gval = c._adjoint(self.back, self.lam, g, self.p[g])
-            self.grads[g] = 2.0 * (self.ov.conj() * gval).imag
+        for g, n in reversed(c._steps):
+            c._adjoint_step(self.back, self.lam, g, n, self.p, self.gvals)
             ck = self.ck.get(g)
             if ck is not None:
                 self.back.copy_(ck)
+        self.grads.copy_(2.0 * (self.ov.conj()[None, :] * self.gvals).imag)
 
 
 class _GraphFidelityLoss(torch.autograd.Function):

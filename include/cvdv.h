@@ -217,6 +217,17 @@ int cvdvBatchRxAdjoint(void* psi, void* lam, int precision, int batch, int n, in
                        double* gOut, void* stream);
 int cvdvBatchCondDispAdjoint(void* psi, void* lam, int precision, int batch, int n, int modeQubits,
                              int ctrlBit, const double* betas, double* gOut, void* stream);
+/* A layer Rx(thetas[b]) on flat bit `bit` followed by cd(betas[b]) controlled by
+ * the same bit, on a mode of modeQubits (9..12) bits, as one pass (a cluster of
+ * two CTAs per pair of rows that differ in the bit).  Equal to cvdvBatchRx then
+ * cvdvBatchCondDisp with sign +1. */
+int cvdvBatchRxCondDisp(void* states, int precision, int batch, int n, int modeQubits, int bit,
+                        const double* thetas, const double* betas, void* stream);
+/* Adjoint of that layer: cvdvBatchCondDispAdjoint then cvdvBatchRxAdjoint in one
+ * pass, writing g for the cd to gCd and for the Rx to gRx (as gOut above). */
+int cvdvBatchRxCondDispAdjoint(void* psi, void* lam, int precision, int batch, int n, int modeQubits, int bit,
+                               const double* thetas, const double* betas, double* gRx, double* gCd,
+                               void* stream);
 /* out[2b], out[2b+1] = <target| states_b> (target shared by every instance, or
  * one per instance when targetPerInstance != 0). */
 int cvdvBatchOverlap(const void* states, const void* target, int precision, int batch, int n,

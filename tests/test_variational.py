@@ -171,6 +171,49 @@ def test_full_config_gradient_step():
     assert err < 1e-3, err
 
 
+@pytest.mark.parametrize("precision,qubits,tol", [("complex128", [1, 12], 1e-13), ("complex64", [1, 12], 2e-6),
+                                                   ("complex128", [2, 9], 1e-13), ("complex64", [2, 10], 2e-6)])
+def test_fused_layer_matches_separate_gates(precision, qubits, tol):
+    """cvdvBatchRxCondDisp equals cvdvBatchRx then cvdvBatchCondDisp, and its adjoint
+    equals the cd adjoint then the Rx adjoint (states and g values), on random
+    states of a batch; the control is each qubit bit in turn."""
+    import ctypes
+    from cvdv_b200 import _lib
+    L = _lib.load()
+    prec = 0 if precision == "complex128" else 1
+    cdt = torch.complex128 if prec == 0 else torch.complex64
+    B, n, q = 5, sum(qubits), qubits[-1]
+    rng = np.random.default_rng(n)
+    ptr = lambda t: ctypes.c_void_p(t.data_ptr())
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def rnd():
+        a = rng.standard_normal((B, 1 << n)) + 1j * rng.standard_normal((B, 1 << n))
+        return torch.tensor(a / np.linalg.norm(a, axis=1, keepdims=True), dtype=cdt, device="cuda")
+
+    th = torch.tensor(rng.uniform(0, 2 * np.pi, B), dtype=torch.float64, device="cuda")
+    be = torch.tensor(rng.normal(0, 0.5, B), dtype=torch.float64, device="cuda")
+    for bit in range(q, n):
+        psi, lam = rnd(), rnd()
+        a, b = psi.clone(), psi.clone()
+        assert L.cvdvBatchRx(ptr(a), prec, B, n, bit, ptr(th), 1.0, stream) == 0
+        assert L.cvdvBatchCondDisp(ptr(a), prec, B, n, q, bit, ptr(be), 1.0, stream) == 0
+        assert L.cvdvBatchRxCondDisp(ptr(b), prec, B, n, q, bit, ptr(th), ptr(be), stream) == 0
+        torch.cuda.synchronize()
+        assert float((a - b).abs().max()) < tol, bit
+        pa, la, pb, lb = psi.clone(), lam.clone(), psi.clone(), lam.clone()
+        gcd, grx = (torch.zeros(2 * B, dtype=torch.float64, device="cuda") for _ in range(2))
+        gcd2, grx2 = (torch.zeros(2 * B, dtype=torch.float64, device="cuda") for _ in range(2))
+        assert L.cvdvBatchCondDispAdjoint(ptr(pa), ptr(la), prec, B, n, q, bit, ptr(be), ptr(gcd), stream) == 0
+        assert L.cvdvBatchRxAdjoint(ptr(pa), ptr(la), prec, B, n, bit, ptr(th), ptr(grx), stream) == 0
+        assert L.cvdvBatchRxCondDispAdjoint(ptr(pb), ptr(lb), prec, B, n, q, bit, ptr(th), ptr(be), ptr(grx2),
+                                            ptr(gcd2), stream) == 0
+        torch.cuda.synchronize()
+        assert float((pa - pb).abs().max()) < tol and float((la - lb).abs().max()) < tol, bit
+        assert float((gcd - gcd2).abs().max()) < 10 * tol * (1 + float(gcd.abs().max())), bit
+        assert float((grx - grx2).abs().max()) < 10 * tol, bit
+
+
 def test_graph_replay_matches_eager():
     """graphs=True (both sweeps captured once and replayed) gives the eager losses and
     gradients, on two steps in a row with different parameters."""
