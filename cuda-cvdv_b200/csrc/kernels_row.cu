@@ -676,13 +676,15 @@ static cudaError_t launch_rowr(Context* ctx, const RowProgram& P, int q) {
 }
 
 // A program on a register that is not the last one runs on k_rowr in column
-// form for complex64 registers of 2^9 .. 2^14 points (at least as many columns as
-// one CTA takes).  The column loads are strided, but one pass replaces the two
-// per transform of the column kernel; in complex128 the column kernel measured
-// faster, and registers of up to 2^8 points run whole on it anyway.
+// form for registers of 2^9 .. 2^14 (complex64) or 2^13 (complex128) points, at
+// least as many columns as one CTA takes.  The column loads are strided, but one
+// pass replaces the two per transform of the column kernel (with the linear-phase
+// runs taken without tables this also wins in complex128: 5.1 against 5.7 ms of
+// column work per [13, 13] layer); registers of up to 2^8 points run whole on the
+// column kernel anyway.
 bool col_program_ok(Context* ctx, int reg) {
   const int q = ctx->q[reg];
-  if (!ctx->colProg || ctx->precision != kC64 || ctx->flw[reg] == 0 || q <= 8 ||
+  if (!ctx->colProg || ctx->flw[reg] == 0 || q <= 8 ||
       q > rowr_max_log(ctx->precision))
     return false;
   if (ctx->colFft && col_fft_ok(ctx, reg) && tc_col_ok(ctx, reg)) return false;  // chained tensor-core passes
