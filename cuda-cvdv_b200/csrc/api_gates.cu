@@ -394,6 +394,7 @@ static void release(Context* c) {
   for (auto& b : c->arenaExtra) cudaFree(b.p);
   c->arenaExtra.clear();
   if (c->big) cudaFree(c->big);
+  if (c->rowSumBuf) cudaFree(c->rowSumBuf);
   c->big = nullptr;
   c->bigCap = 0;
   if (c->waitErr) cudaFreeHost(c->waitErr);

@@ -857,7 +857,10 @@ bool flush(Context* ctx) {
     }
     if (op.rowReg >= 0) {
       if (op.blockedIn) ctx->permReg = -1;  // this program reads the blocked layout itself
-      if (!launch_row_program(ctx, op.rowReg, op.row, op.blockedIn, op.blockedOut)) return false;
+      // the flush's last op on the last register may also write the row sums a
+      // marginal readout asked for
+      const bool sums = ctx->rowSums && oi + 1 == ops.size() && op.rowReg == ctx->numReg - 1 && !op.blockedOut;
+      if (!launch_row_program(ctx, op.rowReg, op.row, op.blockedIn, op.blockedOut, sums)) return false;
       if (op.blockedOut) {
         ctx->permReg = op.rowReg;
         ctx->permLogC = rowc_log_cluster();

@@ -289,6 +289,13 @@ struct Context {
   // these tables instead of reading the state (set by flush, taken by launch_seq)
   const double2* seqProdLast = nullptr;
   const double2* seqProdOuter = nullptr;
+  // Set by a marginal readout of registers above the last one before it flushes:
+  // a row program on the last register that ends the flush also writes each
+  // row's sum of |psi|^2 there (rowSumParts partials per row; 0 = not written).
+  double* rowSums = nullptr;
+  int rowSumParts = 0;
+  double* rowSumBuf = nullptr;  // owned buffer for them
+  size_t rowSumCap = 0;         // in doubles
   int nextFtTag = 1;
   long long ftCancelled = 0;
 
@@ -372,7 +379,9 @@ bool launch_col_chain(Context* ctx, int reg, const std::vector<HostRowOp>& ops);
 // blockedIn: the register is stored blocked and the program starts with an
 // inverse transform; blockedOut: leave it blocked after the final forward transform
 bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops, bool blockedIn = false,
-                        bool blockedOut = false);
+                        bool blockedOut = false, bool rowSums = false);
+// largest number of row-sum partials per row a row program writes (32)
+constexpr int kRowSumMaxParts = 32;
 // whether launch_row_program runs this program on the cluster kernel (which can
 // store and load the blocked layout)
 bool rowc_takes(Context* ctx, int reg, const std::vector<HostRowOp>& ops);

@@ -99,6 +99,7 @@ struct RowProgram {
   int storeBlocked;  // cluster rows ending transposed: write the blocked layout
   int logS;          // k_rowr on a strided register: log2 of the amplitudes below it (0: rows)
   const double2* tw;
+  double* rowSums;        // non-null: per-warp partial sums of |psi|^2 of every row's result
   unsigned int* waitErr;  // set when a bounded wait on the cluster peers gives up
   RowOp ops[kMaxRowOps];
   RowDiag diag[kMaxRowDiags];
@@ -579,6 +580,19 @@ __device__ __forceinline__ void l2_prefetch_tile(const void* p, uint32_t bytes) 
 // sits m S amplitudes after its first.  The CTA's columns are adjacent inner
 // indices; a warp's loads hit 32 different sectors, whose other halves the
 // CTAs of the neighbouring columns, running at the same time, read from L2.
+// The sum of |psi|^2 (FP64) over the E amplitudes of each of a group of W lanes
+// (W = 32, or the lanes of one row when a warp holds several), written by the
+// group's first lane.
+template <typename C, int E, int W>
+__device__ __forceinline__ void row_sum_part(const C (&v)[E], double* out) {
+  double a = 0.0;
+#pragma unroll
+  for (int k = 0; k < E; ++k) a += (double)v[k].x * (double)v[k].x + (double)v[k].y * (double)v[k].y;
+#pragma unroll
+  for (int o = W / 2; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+  if ((threadIdx.x & (W - 1)) == 0) *out = a;
+}
+
 template <typename C, int LOGM, int LOGR, int LOGE, bool COL>
 __global__ void __launch_bounds__(1 << (LOGM - LOGE + LOGR), (LOGM - LOGE + LOGR) > 8 ? 1 : 2)
     k_rowr(const C* __restrict__ in, C* __restrict__ out, uint64_t nTiles, const __grid_constant__ RowProgram P) {
@@ -621,6 +635,11 @@ __global__ void __launch_bounds__(1 << (LOGM - LOGE + LOGR), (LOGM - LOGE + LOGR
       if (op.kind == kRowDiag) rr_diag<C, LOGM, LOGE>(v, P.diag[op.diag], rowBase, t);
       else if (op.dir > 0) rr_stages<C, 1, LOGM, 0, LOGE>(v, smrow, t, lo, hi);
       else rr_stages<C, -1, LOGM, 0, LOGE>(v, smrow, t, lo, hi);
+    }
+    if constexpr (!COL) {
+      // the row's |psi|^2 in TPR / 32 partials (one when a warp holds several rows)
+      constexpr int W = TPR < 32 ? TPR : 32, PARTS = TPR < 32 ? 1 : TPR / 32;
+      if (P.rowSums) row_sum_part<C, E, W>(v, P.rowSums + (rowBase >> LOGM) * PARTS + t / 32);
     }
 #pragma unroll
     for (int k = 0; k < E; ++k) out[rowBase + ((uint64_t)(t + k * TPR) << logS)] = v[k];
@@ -998,6 +1017,8 @@ __global__ void __launch_bounds__(1 << (LOGN - LOGC - 4), 1 << (LOGC - 1))
     }
 
     if (arrived) cluster_wait_acquire();  // pair an arrival no exchange waited for
+    // the row's |psi|^2 in C * TPR / 32 partials (one per warp of the cluster)
+    if (P.rowSums) row_sum_part<C, 16, 32>(v, P.rowSums + row * (NC * TPR / 32) + r * (TPR / 32) + t / 32);
     if (!layoutT) {
 #pragma unroll
       for (int k = 0; k < 16; ++k) out[rowBase + (uint64_t)(k / IPS) * M + r * Q + t + TPR * (k % IPS)] = v[k];
@@ -1196,7 +1217,7 @@ bool rowc_takes(Context* ctx, int reg, const std::vector<HostRowOp>& ops) {
 }
 
 bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops, bool blockedIn,
-                        bool blockedOut) {
+                        bool blockedOut, bool rowSums) {
   RowProgram P{};
   // Registers up to the normal tile run two 256-thread CTAs per SM; longer ones
   // use the big tile (512 threads, twice the amplitudes, one CTA per SM) and, past
@@ -1362,6 +1383,10 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
   if (useC && !elemF && alternating) {
     if (blockedIn) P.loadT = 2;
     P.storeBlocked = blockedOut ? 1 : 0;
+    if (rowSums) {
+      P.rowSums = ctx->rowSums;
+      ctx->rowSumParts = 32;  // 8 CTAs x 4 warps
+    }
     cudaError_t er;
     {
       LaunchScope _ls(ctx, kKFft);
@@ -1375,6 +1400,11 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
     if (elemF) {
       set_error(ctx, kErrUnsupported, "row program: per-element factors left for k_rowr");
       return false;
+    }
+    if (rowSums && !col) {
+      const int logE = (ctx->precision == kC64 && q >= 13) ? 5 : 4, tpr = 1 << (q - logE);
+      P.rowSums = ctx->rowSums;
+      ctx->rowSumParts = tpr < 32 ? 1 : tpr / 32;
     }
     cudaError_t er;
     {

@@ -366,6 +366,86 @@ static bool marginals_tiled(Context* ctx, const std::vector<std::vector<int>>& o
   return cuda_ok(ctx, cudaGetLastError(), "marginal launch");
 }
 
+// Marginals of registers above the last one from the row sums the flush's last
+// row program wrote (a row = one value of every register but the last): the rows'
+// partials are added in a fixed order, then one CTA per output bin adds the rows
+// with that register value in a fixed tree.
+__global__ void k_row_total(const double* __restrict__ parts, int P, uint64_t rows, double* __restrict__ tot) {
+  for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (uint64_t)gridDim.x * blockDim.x) {
+    double a = 0.0;
+    for (int p = 0; p < P; ++p) a += parts[r * P + p];
+    tot[r] = a;
+  }
+}
+
+struct RowMarg {
+  int nOut;
+  int shift[kMargMaxOut], q[kMargMaxOut], off[kMargMaxOut];  // register field in the row index; output offset
+};
+
+__global__ void __launch_bounds__(256) k_row_marg(const double* __restrict__ tot, uint64_t rows,
+                                                  const __grid_constant__ RowMarg M, double* __restrict__ out) {
+  int o = 0;
+  while (o + 1 < M.nOut && (int)blockIdx.x >= M.off[o + 1]) ++o;
+  const uint64_t v = (uint64_t)(blockIdx.x - M.off[o]);
+  const int sh = M.shift[o], q = M.q[o];
+  const uint64_t cnt = rows >> q, low = (1ull << sh) - 1;
+  double a = 0.0;
+  for (uint64_t i = threadIdx.x; i < cnt; i += blockDim.x)
+    a += tot[((i & ~low) << q) | (v << sh) | (i & low)];
+  const double2 s = block_sum2(make_double2(a, 0.0));
+  if (threadIdx.x == 0) out[blockIdx.x] = s.x;
+}
+
+static bool marginals_from_rows(Context* ctx, const std::vector<std::vector<int>>& outs, int parts, double* dOut) {
+  const int last = ctx->numReg - 1;
+  const uint64_t rows = ctx->size() >> ctx->q[last];
+  RowMarg M{};
+  int bins = 0;
+  for (const auto& regs : outs) {
+    const int r = regs[0];
+    M.shift[M.nOut] = ctx->flw[r] - ctx->q[last];
+    M.q[M.nOut] = ctx->q[r];
+    M.off[M.nOut++] = bins;
+    bins += 1 << ctx->q[r];
+  }
+  double* tot = (double*)arena_alloc(ctx, rows * sizeof(double));
+  if (!tot) return false;
+  {
+    LaunchScope _ls(ctx, kKReduce);
+    k_row_total<<<(unsigned)((rows + 255) / 256 < 1184 ? (rows + 255) / 256 : 1184), 256, 0, ctx->stream>>>(
+        ctx->rowSumBuf, parts, rows, tot);
+  }
+  {
+    LaunchScope _ls(ctx, kKReduce);
+    k_row_marg<<<bins, 256, 0, ctx->stream>>>(tot, rows, M, dOut);
+  }
+  return cuda_ok(ctx, cudaGetLastError(), "row-sum marginal launch");
+}
+
+// Ask the next flush for row sums when every register read is a single register
+// above the last one; false (nothing asked) otherwise.
+static bool request_row_sums(Context* c, const std::vector<std::vector<int>>& outs) {
+  if (c->numReg < 2 || outs.empty()) return false;
+  for (const auto& regs : outs)
+    if (regs.size() != 1 || regs[0] == c->numReg - 1) return false;
+  const size_t need = (c->size() >> c->q[c->numReg - 1]) * kRowSumMaxParts;
+  if (need > c->rowSumCap) {
+    cudaStreamSynchronize(c->stream);
+    if (c->rowSumBuf) cudaFree(c->rowSumBuf);
+    c->rowSumBuf = nullptr;
+    c->rowSumCap = 0;
+    if (cudaMalloc(&c->rowSumBuf, need * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    c->rowSumCap = need;
+  }
+  c->rowSums = c->rowSumBuf;
+  c->rowSumParts = 0;
+  return true;
+}
+
 static bool tiled_ok(Context* ctx, long long bins) {
   return bins <= kMargSmemBins && ctx->totalQbt >= kMargLogTile;
 }
@@ -591,10 +671,18 @@ void cvdvMeasureEach(CVDVContext* ctx, const int* regIdxs, int numRegs, double* 
   for (size_t k = 0; k < big.size(); ++k)
     if (!measure(c, &big[k], 1, probsOut + bigPos[k], w)) return;
   if (outs.empty()) return;
-  if (!ready(c, w)) return;
+  // qubit registers after a row program on the last register: the program writes
+  // the row sums on its way out and the marginals come from them, not another pass
+  const bool asked = request_row_sums(c, outs);
+  const bool ok = ready(c, w);
+  c->rowSums = nullptr;
+  if (!ok) return;
+  const int parts = asked ? c->rowSumParts : 0;
+  c->rowSumParts = 0;
   arena_reset(c);
   double* dOut = (double*)arena_alloc(c, (size_t)tiledBins * sizeof(double));
-  if (!dOut || !marginals_tiled(c, outs, dOut)) return;
+  if (!dOut) return;
+  if (!(parts > 0 ? marginals_from_rows(c, outs, parts, dOut) : marginals_tiled(c, outs, dOut))) return;
   size_t src = 0;
   for (size_t k = 0; k < outs.size(); ++k) {
     const size_t b = (size_t)1 << c->q[outs[k][0]];

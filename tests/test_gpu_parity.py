@@ -435,6 +435,32 @@ def test_product_formed_in_first_sequence(n_qubits, mode_qubits):
         assert rel(outs[31], outs[15]) < tol
 
 
+@pytest.mark.parametrize("n_qubits,mode_qubits", [(6, 14), (5, 12), (4, 9)])
+def test_marginals_after_row_program(n_qubits, mode_qubits):
+    """mEach of every qubit register straight after a circuit whose flush ends with
+    a row program on the mode: the program writes each row's |psi|^2 and the
+    marginals come from those sums (2^14 rows on the cluster kernel, 2^12 and 2^9
+    on the single-CTA one), equal to the oracle; the same readout after a state
+    read (no pending work) takes the marginal pass."""
+    from cvdv_b200 import CudaCvdv
+    from cvdv_b200 import workloads as W
+    circ = W.state_transfer(n_qubits=n_qubits, mode_qubits=mode_qubits)
+    o = OracleSim(circ["qubits"])
+    o.initStateVector(W.separable_arrays(circ))
+    W.apply(o, circ["prep"] + circ["gates"])
+    ref = [o.m(k) for k in range(n_qubits)]
+    for prec, tol in (("complex128", 1e-12), ("complex64", 2e-6)):
+        sim = CudaCvdv(circ["qubits"], precision=prec, check_errors=True)
+        sim.initStateVector(W.separable_arrays(circ, device="cuda"))
+        W.apply(sim, circ["prep"] + circ["gates"])
+        each = sim.mEach(list(range(n_qubits)))
+        for k in range(n_qubits):
+            np.testing.assert_allclose(each[k], ref[k], atol=tol, err_msg=f"{prec} {k}")
+        again = sim.mEach(list(range(n_qubits)))
+        for k in range(n_qubits):
+            np.testing.assert_allclose(again[k], each[k], atol=tol)
+
+
 def test_transform_cancellation_matches_unfused():
     """Queue cancellation of FtP2Q/FtQ2P pairs changes nothing but rounding."""
     from cvdv_b200 import CudaCvdv, _lib
