@@ -577,9 +577,10 @@ __device__ __forceinline__ void l2_prefetch_tile(const void* p, uint32_t bytes) 
 //
 // With COL the "rows" are the columns of a strided register (P.logS amplitudes
 // below it): column c is inner index c mod S and outer index c / S, and element m
-// sits m S amplitudes after its first.  The CTA's columns are adjacent inner
-// indices; a warp's loads hit 32 different sectors, whose other halves the
-// CTAs of the neighbouring columns, running at the same time, read from L2.
+// sits m S amplitudes after its first.  The CTA's 2^LOGR columns (at least two
+// within 512 threads) are adjacent inner indices interleaved lane by lane, so a
+// warp's load covers runs of 2^LOGR amplitudes; the rest of each sector is read
+// from L2 by the CTAs of the neighbouring columns.
 // The sum of |psi|^2 (FP64) over the E amplitudes of each of a group of W lanes
 // (W = 32, or the lanes of one row when a warp holds several), written by the
 // group's first lane.
@@ -603,8 +604,10 @@ __global__ void __launch_bounds__(1 << (LOGM - LOGE + LOGR), (LOGM - LOGE + LOGR
   double2* lo = reinterpret_cast<double2*>(sm + (RS << LOGR));  // w_M^e, e < 64
   double2* hi = lo + 64;                                         // w_M^(64 h), h < M / 64
   const int tid = threadIdx.x;
-  const int row = tid >> (LOGM - LOGE);
-  const int t = tid & (TPR - 1);
+  // column form: the CTA's 2^LOGR adjacent columns interleave lane by lane, so a
+  // warp's load covers 32 / 2^LOGR points of every column in runs of 2^LOGR
+  const int row = COL ? (tid & ((1 << LOGR) - 1)) : tid >> (LOGM - LOGE);
+  const int t = COL ? (tid >> LOGR) : tid & (TPR - 1);
   C* smrow = sm + row * RS;
   const int logS = COL ? P.logS : 0;
 
@@ -659,7 +662,9 @@ struct RrShape {
 
 template <typename C, int LOGM, bool COL>
 static cudaError_t launch_rowr_t(Context* ctx, const RowProgram& P) {
-  constexpr int LOGE = RrShape<C, LOGM>::LOGE, LOGR = RrShape<C, LOGM>::LOGR;
+  constexpr int LOGE = RrShape<C, LOGM>::LOGE, LOGR0 = RrShape<C, LOGM>::LOGR;
+  // column form: at least two columns a CTA while it stays within 512 threads
+  constexpr int LOGR = (COL && LOGR0 == 0 && (LOGM - LOGE) < 9) ? 1 : LOGR0;
   constexpr int NT = 1 << (LOGM - LOGE + LOGR);
   constexpr int M = 1 << LOGM;
   const size_t smem = (size_t)(M + (M >> 4)) * (1 << LOGR) * sizeof(C) + (64 + (M >> 6)) * sizeof(double2);
@@ -708,7 +713,7 @@ bool col_program_ok(Context* ctx, int reg) {
     return false;
   if (ctx->colFft && col_fft_ok(ctx, reg) && tc_col_ok(ctx, reg)) return false;  // chained tensor-core passes
   const int logE = (ctx->precision == kC64 && q >= 13) ? 5 : 4;
-  const int logR = q - logE < 8 ? 8 - (q - logE) : 0;
+  const int logR = q - logE < 8 ? 8 - (q - logE) : (q - logE < 9 ? 1 : 0);
   return ctx->totalQbt - q >= logR;
 }
 
