@@ -54,9 +54,10 @@ def peaks():
 
 class Clocks:
     """SM clock and clock-event reasons sampled DURING the timed region: NVML read
-    every 5 ms from a background thread (the region lasts tens of milliseconds, too
-    short for nvidia-smi's sampling); nvidia-smi at 200 ms if NVML is missing.
-    Read-only queries: no clock or power setting is touched."""
+    every 5 ms from a background thread and every 2 ms from the timing loop while it
+    waits for the timed steps (the region lasts tens of milliseconds, too short for
+    nvidia-smi's sampling); nvidia-smi at 200 ms if NVML is missing.  Read-only
+    queries: no clock or power setting is touched."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -77,17 +78,23 @@ class Clocks:
         except Exception:
             self.nvml = None
 
-    def _poll(self):
+    def sample(self):
+        """One NVML reading (also called from the timing loop while the GPU works)."""
         nv = self.nvml
+        if nv is None:
+            return
+        try:
+            sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+            smax = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+            get = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            self.samples.append((sm, smax, int(get(self.h))))
+        except Exception:
+            pass
+
+    def _poll(self):
         while not self.done:
-            try:
-                sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
-                smax = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
-                get = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
-                    nv.nvmlDeviceGetCurrentClocksThrottleReasons
-                self.samples.append((sm, smax, int(get(self.h))))
-            except Exception:
-                pass
+            self.sample()
             time.sleep(0.005)
 
     def start(self):
@@ -113,7 +120,7 @@ class Clocks:
             reasons = sorted(k for k, bit in self.REASONS.items() if any(x[2] & bit for x in self.samples))
             return {"sm_mhz": statistics.median(sm) if sm else None,
                     "sm_max_mhz": max(x[1] for x in self.samples) if sm else None,
-                    "reasons": reasons, "samples": len(sm), "source": "nvml, 5 ms"}
+                    "reasons": reasons, "samples": len(sm), "source": "nvml, 2-5 ms"}
         if self.p is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         time.sleep(0.3)
@@ -281,6 +288,9 @@ def run_gpu(args, world, rank, local):
             W.apply(sim, circ["gates"])
             L.cvdvFlush(sim.ctx)
         e1.record(stream)
+        while not e1.query():  # read the clocks while the timed steps run on the GPU
+            clk.sample()
+            time.sleep(0.002)
         e1.synchronize()
         clocks = clk.stop()
         launches = L.cvdvLaunchCount() - n0
