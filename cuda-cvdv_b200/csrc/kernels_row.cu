@@ -740,20 +740,32 @@ bool col_program_ok(Context* ctx, int reg) {
 // receiving CTA's shared memory (slot (I src + i) TPR + t); the I it keeps never
 // leave its registers.  Diagonal runs in T read tables stored permuted for C CTAs
 // (position r M + k2 holds index r + C k2).
-template <typename C, int LOGM, int LOGC>
+// XX: the run may hold bilinear terms (D.nLin); programs without them use the
+// instantiation that has no code for them.
+template <typename C, int LOGM, int LOGC, bool XX>
 __device__ __forceinline__ void rq_diag(C (&v)[16], const RowDiag& D, uint64_t rowBase, int t, int r,
                                         bool layoutT) {
   constexpr int M = 1 << LOGM, TPR = M / 16, IPS = 16 >> LOGC, Q = M >> LOGC, NC = 1 << LOGC;
   constexpr long long N = (long long)M << LOGC;
   const double2 rs = D.hasRowF ? eval_factor(D.rowF, rowBase) : make_double2(1.0, 0.0);
-  if (D.ftSign || D.nPl) {
+  const bool lin = D.ftSign || D.nPl || (XX && D.nLin);
+  if (lin) {
     // linear phases as running products from values at a thread's first point (a
     // thread's points are arithmetic progressions in n): T holds
     // n = r + C (t + TPR w), S holds n = j1 M + r Q + t + TPR i at v[I j1 + i].
-    // The transform twiddle's values are exact (integer-reduced angles).
+    // The transform twiddle's values are exact (integer-reduced angles); c x terms
+    // and bilinear terms with other registers add to one coefficient of x.
     double c = 0.0;
     for (int k = 0; k < D.nPl; ++k)
       c += (D.plCtrl[k] >= 0 && ((rowBase >> D.plCtrl[k]) & 1ull)) ? -D.plC[k] : D.plC[k];
+    if constexpr (XX)
+      for (int l = 0; l < D.nLin; ++l) {
+        const XXFactor& X = D.lin[l];
+        const int j = (int)((rowBase >> X.shift1) & (uint64_t)X.mask1);
+        double cc = X.coeff * (((double)j - X.c1) * X.dx1);
+        if (X.ctrlShift >= 0 && ((rowBase >> X.ctrlShift) & 1ull)) cc = -cc;
+        c += cc;
+      }
     c *= D.regDx;
     auto at = [&](long long n) {
       double2 f = D.ftSign ? ft_tw_at(n, N, D.ftSign) : make_double2(1.0, 0.0);
@@ -795,7 +807,7 @@ __device__ __forceinline__ void rq_diag(C (&v)[16], const RowDiag& D, uint64_t r
         f = dmul(f, sj);
       }
     }
-    return;
+    if constexpr (!XX) return;  // (without bilinear terms a run is linear or tabled)
   }
   if (D.tab) {
     int seg = 0;
@@ -813,11 +825,11 @@ __device__ __forceinline__ void rq_diag(C (&v)[16], const RowDiag& D, uint64_t r
       }
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
-        if (D.hasRowF) w[k] = dmul(w[k], rs);
+        if (D.hasRowF && !(XX && lin)) w[k] = dmul(w[k], rs);  // (a linear pass carried rs)
         v[k0 + k] = cmul(v[k0 + k], fromd<C>(w[k]));
       }
     }
-  } else if (D.hasRowF) {
+  } else if (D.hasRowF && !(XX && lin)) {
     const C c = fromd<C>(rs);
 #pragma unroll
     for (int k = 0; k < 16; ++k) v[k] = cmul(v[k], c);
@@ -925,7 +937,7 @@ __device__ __forceinline__ void rq_cross(C (&v)[16], int i, const double2* loN, 
   for (int j = 0; j < NC; ++j) v[IPS * j + i] = DIR > 0 ? cmul(a[j], w[j]) : a[j];
 }
 
-template <typename C, int LOGN, int LOGC>
+template <typename C, int LOGN, int LOGC, bool XX>
 __global__ void __launch_bounds__(1 << (LOGN - LOGC - 4), 1 << (LOGC - 1))
     k_rowq(const C* __restrict__ in, C* __restrict__ out, uint64_t nRows, const __grid_constant__ RowProgram P) {
   constexpr int LOGM = LOGN - LOGC, M = 1 << LOGM, TPR = M / 16, NC = 1 << LOGC, IPS = 16 >> LOGC, Q = M >> LOGC;
@@ -993,7 +1005,7 @@ __global__ void __launch_bounds__(1 << (LOGN - LOGC - 4), 1 << (LOGC - 1))
     for (int o = 0; o < P.nOps; ++o) {
       const RowOp& op = P.ops[o];
       if (op.kind == kRowDiag) {
-        rq_diag<C, LOGM, LOGC>(v, P.diag[op.diag], rowBase, t, r, layoutT);
+        rq_diag<C, LOGM, LOGC, XX>(v, P.diag[op.diag], rowBase, t, r, layoutT);
       } else if (op.dir > 0) {  // S -> T
 #pragma unroll
         for (int i = 0; i < IPS; ++i) rq_cross<C, 1, LOGC>(v, i, loN, hiN, r * Q + t + TPR * i);
@@ -1038,11 +1050,11 @@ __global__ void __launch_bounds__(1 << (LOGN - LOGC - 4), 1 << (LOGC - 1))
     // reads of it (the last exchange or stage) ended in a CTA barrier.
   }
 }
-template <typename C, int LOGN, int LOGC>
+template <typename C, int LOGN, int LOGC, bool XX>
 static cudaError_t launch_rowq_t(Context* ctx, const RowProgram& P) {
   constexpr int M = 1 << (LOGN - LOGC), NC = 1 << LOGC;
   const size_t smem = (size_t)(M + (M >> 4)) * sizeof(C) + 2 * (64 + (M >> 6)) * sizeof(double2);
-  auto kern = k_rowq<C, LOGN, LOGC>;
+  auto kern = k_rowq<C, LOGN, LOGC, XX>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess && NC > 8) e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   if (e != cudaSuccess) return e;
@@ -1193,7 +1205,9 @@ static cudaError_t launch_row_t(Context* ctx, const RowProgram& P, uint64_t nCta
 
 // 2^14-point complex128 rows run on the eight-CTA kernel (k_rowq).  Complex64 rows
 // of that length fit one CTA, k_rowr, which measured faster for them than k_rowq
-// (2.0 against 1.5 ms per 2^28-amplitude launch).
+// (1.43 against 1.61 ms per 2^28-amplitude launch); so did the one-CTA k_rowr for
+// 2^13-point complex128 rows against a four-CTA k_rowq (3.30 against 3.41 ms of
+// row programs per layer of the two-mode [13, 13] network).
 static bool rowc_shape(Context* ctx, int reg, const std::vector<HostRowOp>& ops) {
   if (ctx->precision != kC128 || ctx->q[reg] != 14 || !row_eligible(ctx, reg)) return false;
   int lastDir = 0;
@@ -1215,7 +1229,8 @@ bool rowc_takes(Context* ctx, int reg, const std::vector<HostRowOp>& ops) {
     if (h.kind != kRowDiag) continue;
     std::vector<Term> regTerms, rowTerms, elemTerms;
     std::vector<int> bits;
-    if (!split_row_diag(ctx, reg, h.terms, &regTerms, &bits, &rowTerms, &elemTerms) || !elemTerms.empty())
+    if (!split_row_diag(ctx, reg, h.terms, &regTerms, &bits, &rowTerms, &elemTerms) ||
+        !all_linear(ctx, reg, elemTerms) || elemTerms.size() > (size_t)kMaxXX)
       return false;
   }
   return true;
@@ -1338,7 +1353,7 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
       D.tab = tab;
     }
     D.nLin = 0;
-    if (toRowr) {
+    if (toRowr || useC) {
       const int lo = ctx->flw[reg];
       std::vector<Term> rest;
       for (const Term& t : elemTerms) {
@@ -1395,7 +1410,9 @@ bool launch_row_program(Context* ctx, int reg, const std::vector<HostRowOp>& ops
     cudaError_t er;
     {
       LaunchScope _ls(ctx, kKFft);
-      er = launch_rowq_t<double2, 14, 3>(ctx, P);
+      bool xx = false;
+      for (int d = 0; d < P.nDiag; ++d) xx |= P.diag[d].nLin > 0;
+      er = xx ? launch_rowq_t<double2, 14, 3, true>(ctx, P) : launch_rowq_t<double2, 14, 3, false>(ctx, P);
     }
     if (!cuda_ok(ctx, er, "row program launch")) return false;
     ctx->cur ^= 1;

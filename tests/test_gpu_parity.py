@@ -362,7 +362,8 @@ def _random_multimode_circuit(rng, qubits, n_gates):
     return seq
 
 
-@pytest.mark.parametrize("qubits", [[2, 9, 9], [1, 8, 6, 5], [2, 13, 5], [1, 5, 12], [1, 6, 14]])
+@pytest.mark.parametrize("qubits", [[2, 9, 9], [1, 8, 6, 5], [2, 13, 5], [1, 5, 12], [1, 6, 14], [1, 5, 13],
+                                    [2, 6, 13]])
 def test_random_multimode_circuits(qubits):
     """Random circuits over several modes: the planner's look-ahead (programs that
     jump over commuting stages), column chains and row programs against the oracle,
