@@ -141,22 +141,96 @@ bool launch_build_table(Context* ctx, int r, bool ctrl, const Term* terms, int n
 }
 
 // ----------------------------------------------------------------- diag run
+// A thread takes V = 4 amplitudes i0 + 256 k with i0 a multiple of 1024 plus the
+// thread index: its indices differ only in bits 8-9, which hold k.  A register
+// field that misses those bits has the same index for all four, so its table
+// entry is loaded once; a field that contains both (and reaches bit 8 or lower)
+// advances by 2^(8 - shift) per k, so a bilinear term c x_r x_s whose sides are
+// each fixed or advancing (and whose control, if any, is not bit 8 or 9) is
+// linear in k: its value at k = 0 and the ratio between steps, two sincos,
+// replace the four per-amplitude ones.  Other factors are evaluated per amplitude.
 template <typename C>
 __global__ void __launch_bounds__(256) k_diag(C* __restrict__ st, uint64_t n, FactorList F) {
-  constexpr int V = 4;
-  uint64_t stride = (uint64_t)gridDim.x * blockDim.x * V;
-  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x * V + threadIdx.x; base < n;
-       base += stride) {
+  constexpr int V = 4;  // 256 threads x V amplitudes span bits 0..9
+  // -1: the field holds one of bits 8, 9 only; 0: neither; else the step per k
+  auto field = [](int shift, int mask) -> int {
+    const int q = __popc(mask);
+    if (shift >= 10 || shift + q <= 8) return 0;
+    return (shift <= 8 && shift + q >= 10) ? (1 << (8 - shift)) : -1;
+  };
+  auto ctrl_fixed = [](int c) { return c < 8 || c > 9; };  // (-1: no control)
+  const uint64_t stride = (uint64_t)gridDim.x * 256 * V;
+  for (uint64_t base = (uint64_t)blockIdx.x * 256 * V + threadIdx.x; base < n; base += stride) {
     C v[V];
 #pragma unroll
     for (int k = 0; k < V; ++k) {
-      uint64_t i = base + (uint64_t)k * blockDim.x;
+      const uint64_t i = base + (uint64_t)k * 256;
       if (i < n) v[k] = st[i];
+    }
+    double2 g[V];
+#pragma unroll
+    for (int k = 0; k < V; ++k) g[k] = F.hasScalar ? F.scalar : make_double2(1.0, 0.0);
+#pragma unroll
+    for (int t = 0; t < kMaxTab; ++t) {
+      if (t >= F.nTab) break;
+      const TabFactor& T = F.tab[t];
+      if (field(T.shift, T.mask) == 0 && ctrl_fixed(T.ctrlShift)) {
+        int j = (int)((base >> T.shift) & (uint64_t)T.mask);
+        if (T.ctrlShift >= 0) j += (int)((base >> T.ctrlShift) & 1ull) * T.half;
+        const double2 a = __ldg(T.ptr + j);
+#pragma unroll
+        for (int k = 0; k < V; ++k) g[k] = dmul(g[k], a);
+      } else {
+        double2 a[V];
+#pragma unroll
+        for (int k = 0; k < V; ++k) {
+          const uint64_t i = base + (uint64_t)k * 256;
+          int j = (int)((i >> T.shift) & (uint64_t)T.mask);
+          if (T.ctrlShift >= 0) j += (int)((i >> T.ctrlShift) & 1ull) * T.half;
+          a[k] = __ldg(T.ptr + j);
+        }
+#pragma unroll
+        for (int k = 0; k < V; ++k) g[k] = dmul(g[k], a[k]);
+      }
+    }
+#pragma unroll 1
+    for (int x = 0; x < F.nXX; ++x) {
+      const XXFactor& X = F.xx[x];
+      const int s1 = field(X.shift1, X.mask1), s2 = field(X.shift2, X.mask2);
+      if (s1 >= 0 && s2 >= 0 && ctrl_fixed(X.ctrlShift)) {
+        const double x1 = ((double)((base >> X.shift1) & (uint64_t)X.mask1) - X.c1) * X.dx1;
+        const double x2 = ((double)((base >> X.shift2) & (uint64_t)X.mask2) - X.c2) * X.dx2;
+        double c = X.coeff;
+        if (X.ctrlShift >= 0 && ((base >> X.ctrlShift) & 1ull)) c = -c;
+        // (the two registers differ, so at most one side advances)
+        const double d = s1 ? c * ((double)s1 * X.dx1) * x2 : s2 ? c * x1 * ((double)s2 * X.dx2) : 0.0;
+        double sn, cs;
+        sincos(c * x1 * x2, &sn, &cs);
+        double2 e = make_double2(cs, sn), stp;
+        sincos(d, &stp.y, &stp.x);
+#pragma unroll
+        for (int k = 0; k < V; ++k) {
+          g[k] = dmul(g[k], e);
+          e = dmul(e, stp);
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < V; ++k) {
+          const uint64_t i = base + (uint64_t)k * 256;
+          const double x1 = ((double)((i >> X.shift1) & (uint64_t)X.mask1) - X.c1) * X.dx1;
+          const double x2 = ((double)((i >> X.shift2) & (uint64_t)X.mask2) - X.c2) * X.dx2;
+          double ph = X.coeff * x1 * x2;
+          if (X.ctrlShift >= 0 && ((i >> X.ctrlShift) & 1ull)) ph = -ph;
+          double sn, cs;
+          sincos(ph, &sn, &cs);
+          g[k] = dmul(g[k], make_double2(cs, sn));
+        }
+      }
     }
 #pragma unroll
     for (int k = 0; k < V; ++k) {
-      uint64_t i = base + (uint64_t)k * blockDim.x;
-      if (i < n) st[i] = cmul(v[k], fromd<C>(eval_factor(F, i)));
+      const uint64_t i = base + (uint64_t)k * 256;
+      if (i < n) st[i] = cmul(v[k], fromd<C>(g[k]));
     }
   }
 }

@@ -660,6 +660,39 @@ def test_identities_reference_core():
     assert abs(sim.getFidelity(sep) - 1) < 1e-10
 
 
+@pytest.mark.parametrize("qubits,pairs", [([12, 11], [(0, 1)]), ([9, 4, 10], [(0, 2), (0, 1)]),
+                                          ([10, 8], [(0, 1)]), ([3, 9, 9], [(1, 2)]), ([6, 8, 4], [(1, 0)]),
+                                          ([6, 5, 4], [(1, 0), (2, 0)])])
+def test_standalone_diagonal_runs(qubits, pairs):
+    """Bilinear, shear and cubic phases with nothing to fold them into run as one
+    diagonal pass.  A thread's amplitudes differ in index bits 8-9: registers that
+    miss those bits (one table load, a fixed side of a bilinear term), registers
+    that contain both (a side advancing by 2^(8 - shift): the bilinear term as a
+    running product) and registers that hold only one of them (per amplitude),
+    against the oracle in both precisions."""
+    from cvdv_b200 import _lib
+    L = _lib.load()
+    rng = np.random.default_rng(sum(qubits) * 5 + len(pairs))
+    n = sum(qubits)
+    psi = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    psi /= np.linalg.norm(psi)
+    seq = [("q1q2", (a, b, 0.1 + 0.05 * k)) for k, (a, b) in enumerate(pairs)]
+    seq += [("sheer", (pairs[0][0], 0.05)), ("phaseCubic", (pairs[0][1], 0.01))]
+    o = oracle(qubits, psi)
+    run(o, seq)
+    ref = o.get_state()
+    for prec, tol in (("complex128", PLAIN_TOL), ("complex64", MIXED_TOL)):
+        sim = make(qubits, psi, prec)
+        L.cvdvSetTiming(sim.ctx, 1)
+        _lib.kernel_stats(sim.ctx)
+        run(sim, seq)
+        L.cvdvFlush(sim.ctx)
+        stats = _lib.kernel_stats(sim.ctx)
+        L.cvdvSetTiming(sim.ctx, 0)
+        assert stats["diag"][1] >= 1, stats
+        assert rel(sim.getState(), ref) < tol, prec
+
+
 def test_errors_leave_state_untouched():
     from cvdv_b200 import CudaCvdv
     from cvdv_b200 import _lib
